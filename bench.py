@@ -1,0 +1,415 @@
+"""Throughput benchmark of the 3D FDTD hot path (Gcell-updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1|c3]
+
+A bench step is one complete simulation of the workload: zero the fields,
+run all its leapfrog steps with probe recording.  Default workload (c2):
+128^3 cells, FP32, 1000 leapfrog steps, 10-cell CPML (m=3, R0=1e-6),
+eps_r=4 sphere of radius 20 cells at a seeded offset, Gaussian-modulated Ez
+dipole at the centre (f0 = 0.05/dt, width 30 steps), 16 seeded Ez probes.
+Inputs are synthetic (seeded); no dataset is involved.
+
+`value` times the device work with the inputs resident in HBM; `e2e` times
+the same simulation through the public Python API with host buffers (the
+permittivity map goes in from pinned host memory, the probe traces come
+back to the host) every step.  L2 is flushed (a 256 MiB write) between timed
+steps; each step is bracketed by CUDA events on the launching stream.
+
+--impl reference times the CPU restatement of the reference algorithm
+(oracle/cpu_fdtd.c, FP64, every host thread) on a bounded sample of the
+same workload; under torchrun only rank 0 runs it.
+
+With --gpus N > 1 (torchrun, one process per GPU) every rank runs its own
+independent grid of the same workload (grids do not exchange data), so the
+scaling is weak and `value` sums the cell updates of all ranks over the
+slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (n, leapfrog steps, pml layers, description)
+    "c2": (128, 1000, 10, "fdtd3d-128^3-cpml10-sphere-eps4-pulse-16probes"),
+    "c1": (64, 500, 8, "fdtd3d-64^3-cpml8-vacuum-pulse-8probes"),
+    "c3": (512, 200, 12, "fdtd3d-512^3-cpml12-smoothnoise-eps1to12"),
+}
+
+# DRAM bytes per launch of the dominant kernel from an ncu capture of the same
+# workload (profiles/k3d_tma_cpml_128cubed.md); None until captured.
+NCU_TRAFFIC = {"c2": None, "c1": None, "c3": None}
+
+
+def make_inputs(name: str, seed: int = 0):
+    """Permittivity map, source and probes of a workload (seeded)."""
+    n, steps, pml, _ = WORKLOADS[name]
+    rng = np.random.default_rng(seed + 2)
+    if name == "c2":
+        c = np.array([n // 2] * 3) + rng.integers(-16, 17, size=3)
+        ix, iy, iz = np.ogrid[:n, :n, :n]
+        mask = (ix - c[0]) ** 2 + (iy - c[1]) ** 2 + (iz - c[2]) ** 2 <= 20 ** 2
+        eps = np.where(mask, 4.0, 1.0)
+        n_probes = 16
+    elif name == "c1":
+        eps = None
+        n_probes = 8
+    else:
+        from scipy.ndimage import gaussian_filter
+
+        u = gaussian_filter(rng.random((n, n, n), dtype=np.float32), sigma=6, mode="wrap")
+        u = (u - u.min()) / (u.max() - u.min())
+        eps = 1.0 + 11.0 * u
+        n_probes = 16
+    prng = np.random.default_rng(seed + 1)
+    probes = [tuple(int(v) for v in prng.integers(n // 8, n - n // 8, size=3))
+              for _ in range(n_probes)]
+    return eps, probes
+
+
+def psi_bytes_per_cell(n: int, pml: int) -> float:
+    """CPML psi traffic per cell update: 12 psi arrays, each read and written
+    (8 B) over its slab storage (2*(pml+1) planes of n^2 cells)."""
+    P = pml + 1
+    frac = min(2 * P, n) / n
+    return 12 * frac * 8.0
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+
+    from jaxphys_b200 import CPMLSpec, EMGrid3D, PointSource3D
+
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    n, nsteps, pml, wname = WORKLOADS[args.workload]
+    eps, probes = make_inputs(args.workload, seed=rank)
+    g = EMGrid3D(size=(n, n, n), resolution=1.0, boundary="cpml", pml_layers=pml,
+                 cpml=CPMLSpec(order=3.0, r0=1e-6), device=local)
+    dt = g.default_dt()
+    g.add_source(PointSource3D(frequency=0.05 / dt, position=(n // 2, n // 2, n // 2),
+                               waveform="gauss_sine", width_steps=30.0))
+    for p in probes:
+        g.add_probe(p, "ez")
+    if eps is not None:
+        g.set_permittivity(eps)
+    g.prepare(dt=dt)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def one_step():
+        g.reset()
+        return g.run(nsteps)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(args.warmup):
+        one_step()
+    g.check()
+    barrier()
+
+    # ---- device-resident timing: K steps, L2 flushed between them
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    barrier()
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(stream)
+        g.reset()
+        kev[k][0].record(stream)
+        g.run(nsteps)
+        kev[k][1].record(stream)
+        ev[k][1].record(stream)
+    barrier()
+    clocks = sampler.stop()
+    g.check()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    kern_ms = [a.elapsed_time(b) for a, b in kev]
+    total_ms = float(sum(step_ms))
+    if pg is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # ---- end to end through the public API with host buffers
+    eps_host = None
+    if eps is not None:
+        eps_host = torch.from_numpy(np.ascontiguousarray(eps, dtype=np.float32)).pin_memory()
+    eps_dev = torch.empty((n, n, n), dtype=torch.float32, device=dev)
+    probe_host = torch.empty((nsteps, len(probes)), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        if eps_host is not None:
+            eps_dev.copy_(eps_host, non_blocking=True)
+            g.set_permittivity_device(eps_dev)
+        g.reset()
+        tr = g.run(nsteps)
+        probe_host.copy_(tr, non_blocking=True)
+        return tr
+
+    e2e_step()
+    barrier()
+    e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        e_ev[k][0].record(stream)
+        e2e_step()
+        e_ev[k][1].record(stream)
+    barrier()
+    e2e_ms = float(sum(a.elapsed_time(b) for a, b in e_ev))
+    if pg is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = 0 if eps_host is None else eps_host.numel() * 4
+    d2h = probe_host.numel() * 4
+
+    cells = n ** 3
+    updates = cells * nsteps * args.steps * world
+    value = updates / (total_ms * 1e-3) / 1e9
+    e2e_value = updates / (e2e_ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel (the fused TMA step)
+    info = g.info()
+    per_launch_ms = statistics.mean(kern_ms) / (nsteps + 1)
+    b_cell = 52.0 + psi_bytes_per_cell(n, pml) if eps is not None else 48.0 + psi_bytes_per_cell(n, pml)
+    bytes_per_launch = cells * b_cell
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = NCU_TRAFFIC.get(args.workload)
+
+    line = {
+        "metric": "FDTD3D Gcell-updates/s",
+        "value": round(value, 3),
+        "unit": "Gcell/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded eps_r sphere, pulsed dipole, seeded probes)",
+        "config": {"workload": wname, "cells": cells, "leapfrog_steps_per_step": nsteps,
+                   "boundary": "cpml", "pml_layers": pml, "l2": "flushed (256 MiB write) between steps",
+                   "path": "tma" if info["path"] == 2 else "generic",
+                   "tile": [info["tile_z"], info["tile_y"], info["rows_per_thread"],
+                            info["stages"], info["x_chunk"]],
+                   "parallelism": f"independent grid per GPU x{world}"},
+        "e2e": {"value": round(e2e_value, 3), "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": peak_kind, "bytes_per_cell_update": round(b_cell, 2),
+                     "kernel": "k3d_tma (fused H+E step, CPML)",
+                     "launch_ms": round(per_launch_ms, 5)},
+        "gpu_launches": (nsteps + 1) * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.workload, budget_s=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(workload: str, budget_s: float = 10.0, steps: int | None = None):
+    """The FP64 C restatement of the reference step on every host thread, on a
+    bounded sample (a prefix of the workload's leapfrog steps)."""
+    from oracle import ref_numpy as rn
+    from oracle.cpu_oracle import Oracle3DC, num_threads
+
+    n, nsteps, pml, wname = WORKLOADS[workload]
+    eps, probes = make_inputs(workload)
+    dt = rn.default_dt_3d(1.0)
+    spec = rn.Spec3D(size=(n, n, n), dx=1.0, boundary="cpml", pml_layers=pml, eps_r=eps,
+                     sources=[dict(position=(n // 2,) * 3, polarization="z", amplitude=1.0,
+                                   kind="gauss_sine", frequency=0.05 / dt, width_steps=30.0,
+                                   delay_steps=120.0)],
+                     probes=[p + (2,) for p in probes])
+    o = Oracle3DC(spec, dt=dt)
+    o.run(2)
+    if steps is None:
+        t0 = time.perf_counter()
+        o.run(4)
+        per = (time.perf_counter() - t0) / 4
+        steps = max(4, min(nsteps, int(budget_s / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    o.run(steps)
+    el = time.perf_counter() - t0
+    v = n ** 3 * steps / el / 1e9
+    return {"value": round(v, 4), "unit": "Gcell/s", "cores": num_threads(), "kind": "port",
+            "sample": f"{wname}: leapfrog steps 7..{6 + steps} of {nsteps} (FP64, oracle/cpu_fdtd.c)",
+            "seconds": round(el, 2)}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    n, nsteps, pml, wname = WORKLOADS[args.workload]
+    # each bench step: a bounded sample of the workload on the host cores
+    sample = max(4, min(nsteps, int(os.environ.get("JXF_REF_SAMPLE_STEPS", "20"))))
+    for _ in range(args.warmup):
+        cpu_baseline(args.workload, steps=2)
+    times = []
+    res = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = cpu_baseline(args.workload, steps=sample)
+        times.append(time.perf_counter() - t0)
+    value = statistics.mean([r for r in [res["value"]]])
+    line = {
+        "metric": "FDTD3D Gcell-updates/s",
+        "value": value,
+        "unit": "Gcell/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1e3 * statistics.mean(times), 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded eps_r sphere, pulsed dipole, seeded probes)",
+        "config": {"workload": wname, "cells": n ** 3, "leapfrog_steps_per_step": sample,
+                   "boundary": "cpml", "pml_layers": pml},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "Gcell/s", "cores": res["cores"], "kind": "port",
+                         "sample": res["sample"]},
+        "e2e": {"value": value, "unit": "Gcell/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="c2")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

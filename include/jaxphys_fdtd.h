@@ -1,0 +1,198 @@
+/*
+ * jaxphys_fdtd.h -- C ABI of the B200 (sm_100a) FDTD Maxwell engine.
+ *
+ * Drop-in boundary for the Yee solvers of jaxphys (package `neurosim`):
+ *   3D: src/neurosim/em/fdtd3d.py  (EMGrid3D, PointSource3D, DielectricRegion)
+ *   2D: src/neurosim/em/fdtd.py    (EMGrid, PlaneWave, Wall)
+ * The reference has no native layer: its Python classes call jax.numpy and
+ * jax.lax.scan directly.  Each entry point below replaces the piece of that
+ * Python code cited beside it; a host binding (ctypes, cgo, JNI, N-API) needs
+ * only plain pointers, sizes and integers.
+ *
+ * Conventions
+ *  - Every function returns JXF_OK (0) or a JXF_ERR_* code; the message of the
+ *    last failure on the calling thread is jxf_last_error().
+ *  - Fields are float32, C order (nx, ny, nz) / (nx, ny), z (resp. y) fastest,
+ *    one array per component: the layout of a NumPy / JAX / torch array of
+ *    that shape, so DLPack capsules map 1:1 onto the pointers.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    All device work is ordered on it; nothing synchronises the host except
+ *    the copies to host memory (which synchronise `stream`).
+ *  - A handle owns its device memory (ping-pong field buffers, CPML psi slabs,
+ *    coefficient tables, source/probe tables).  A handle is not thread safe.
+ *  - Component ids: 0..5 = Ex, Ey, Ez, Hx, Hy, Hz (2D: 0..2 = Ez, Hx, Hy).
+ */
+#ifndef JAXPHYS_FDTD_H
+#define JAXPHYS_FDTD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JXF_OK 0
+#define JXF_ERR_INVALID 1    /* bad argument / configuration            */
+#define JXF_ERR_CUDA 2       /* a CUDA runtime / driver call failed      */
+#define JXF_ERR_OOM 3        /* device allocation failed                 */
+#define JXF_ERR_TIMEOUT 4    /* a bounded device wait gave up            */
+#define JXF_ERR_NONFINITE 5  /* NaN / Inf found by jxf_grid3d_check_finite */
+
+/* Boundary modes.  ABSORBING and PERIODIC are the reference's
+ * (fdtd3d.py:94,247-301,361-366; fdtd.py:97,314-352).  PEC is the reference's
+ * non-periodic stencil without the damping multiply (what fdtd3d.py does for
+ * any boundary string other than the two above).  CPML is an extension:
+ * convolutional PML with psi recurrences.  REFLECTING is 2D only
+ * (fdtd.py:264-282). */
+#define JXF_BND_ABSORBING 0
+#define JXF_BND_PERIODIC 1
+#define JXF_BND_PEC 2
+#define JXF_BND_CPML 3
+#define JXF_BND_REFLECTING 4
+
+/* Kernel path selection for 3D grids. */
+#define JXF_PATH_AUTO 0      /* TMA path when the shape allows it          */
+#define JXF_PATH_GENERIC 1   /* plain-load kernels: every mode and shape   */
+#define JXF_PATH_TMA 2       /* TMA-staged marching kernel (nz % 4 == 0,   */
+                             /* boundary != PERIODIC)                       */
+
+typedef struct jxf_grid3d jxf_grid3d;
+typedef struct jxf_grid2d jxf_grid2d;
+
+/* Replaces EMGrid3D.__init__ (fdtd3d.py:90-105) plus the coefficient set-up
+ * of simulate() (fdtd3d.py:185-224: dt, dt/(mu0 dx), dt/(eps0 dx), the PML
+ * sigma profile of :139-167 and its damping factor of :363). */
+typedef struct {
+  int32_t nx, ny, nz;
+  double dx;             /* cell size (m)                                   */
+  double dt;             /* time step (s); <= 0 selects 0.99 dx/(c sqrt 3)  */
+  int32_t boundary;      /* JXF_BND_*                                       */
+  int32_t pml_layers;    /* damping layers (ABSORBING) or CPML thickness    */
+  double cpml_order;     /* CPML polynomial grading m        (default 3)    */
+  double cpml_r0;        /* CPML normal reflection target    (default 1e-6) */
+  double cpml_kappa_max; /* CPML kappa_max                   (default 1)    */
+  double cpml_alpha_max; /* CPML CFS alpha_max, S/m          (default 0)    */
+  int32_t path;          /* JXF_PATH_*                                      */
+  int32_t device;        /* CUDA device ordinal                             */
+} jxf_grid3d_desc;
+
+typedef struct {
+  double dt, coef_h, coef_e;  /* dt, dt/(mu0 dx), dt/(eps0 dx)            */
+  int64_t step;               /* steps taken since the last reset         */
+  int32_t path;               /* JXF_PATH_GENERIC or JXF_PATH_TMA in use  */
+  int32_t tile_z, tile_y, rows_per_thread, stages, x_chunk;
+  int64_t device_bytes;       /* device memory held by the handle         */
+} jxf_grid3d_info;
+
+int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out);
+int jxf_grid3d_destroy(jxf_grid3d* g);
+int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out);
+
+/* Number of TMA launch shapes in the registry, and a way to pin one: cfg in
+ * [0, jxf_num_tma_configs()) and the planes each block marches over;
+ * cfg < 0 returns to autotuning (which runs on the first step otherwise). */
+int jxf_num_tma_configs(void);
+int jxf_grid3d_set_launch(jxf_grid3d* g, int32_t cfg, int32_t x_chunk);
+
+/* Relative permittivity, replaces _build_epsilon_r (fdtd3d.py:132-137) and
+ * the per-cell factor (dt_eps_dx / eps_r) of fdtd3d.py:299,336,345,354.
+ * eps_r: nx*ny*nz float64 values in HOST memory (the library forms
+ * dt/(eps0 dx)/eps_r in FP64 and rounds once), or NULL for vacuum. */
+int jxf_grid3d_set_eps_host(jxf_grid3d* g, const double* eps_r);
+/* Same from a DEVICE float32 array (e.g. a DLPack capsule's data pointer):
+ * the division runs on the device in FP32. */
+int jxf_grid3d_set_eps_device(jxf_grid3d* g, const float* eps_r, void* stream);
+
+/* Soft sources, replaces add_sources (fdtd3d.py:233-245): after the E update
+ * (and damping) of step n, E_comp[cell] += amplitude * wave[wave_id][n].
+ * Entries with the same cell are applied in list order.  cell is the linear
+ * index (ix*ny + iy)*nz + iz, comp in 0..2. */
+int jxf_grid3d_set_sources(jxf_grid3d* g, int32_t n, const int64_t* cell,
+                           const int32_t* comp, const float* amplitude,
+                           const int32_t* wave_id);
+/* Waveform samples for absolute steps 0..n_samples-1 of every wave id
+ * (row-major [n_waves][n_samples], host memory).  The reference's
+ * sin(2 pi f (t0 + n dt)) (fdtd3d.py:238,288) is tabulated by the caller in
+ * FP64. */
+int jxf_grid3d_set_waveforms(jxf_grid3d* g, int32_t n_waves, int64_t n_samples,
+                             const float* samples);
+
+/* Probes (extension): record field comp (0..5) at cell after every step. */
+int jxf_grid3d_set_probes(jxf_grid3d* g, int32_t n, const int64_t* cell,
+                          const int32_t* comp);
+
+/* Advance n_steps leapfrog steps; replaces one jax.lax.scan over `step`
+ * (fdtd3d.py:280-393).  probe_out: DEVICE float32 [n_steps][n_probes] or
+ * NULL.  Returns JXF_ERR_TIMEOUT if a bounded device wait gave up (checked
+ * only when the call synchronises; see jxf_grid3d_check_error). */
+int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stream);
+
+/* Zero fields and psi, reset the step counter. */
+int jxf_grid3d_reset(jxf_grid3d* g, void* stream);
+
+/* Device pointer of the CURRENT buffer of component comp (0..5).  Valid until
+ * the next jxf_grid3d_step (buffers alternate between steps). */
+int jxf_grid3d_field_ptr(jxf_grid3d* g, int32_t comp, float** out);
+/* Copy component comp out of / into the grid.  *_is_host selects host or
+ * device memory for the other side.  Copies to host synchronise `stream`. */
+int jxf_grid3d_get_field(jxf_grid3d* g, int32_t comp, float* dst, int32_t dst_is_host,
+                         void* stream);
+int jxf_grid3d_set_field(jxf_grid3d* g, int32_t comp, const float* src,
+                         int32_t src_is_host, void* stream);
+/* Copy all six components into dst (device, 6*nx*ny*nz floats, component
+ * major): one saved frame of EMFieldHistory3D (fdtd3d.py:371-417). */
+int jxf_grid3d_snapshot(jxf_grid3d* g, float* dst, void* stream);
+
+/* Synchronise `stream` and report a device-side error flag (bounded-wait
+ * timeout) raised by earlier steps; clears the flag. */
+int jxf_grid3d_check_error(jxf_grid3d* g, void* stream);
+/* Synchronise and scan the six fields for NaN/Inf (JXF_ERR_NONFINITE). */
+int jxf_grid3d_check_finite(jxf_grid3d* g, void* stream);
+
+/* ---------------------------------------------------------------- 2D (TM) */
+
+/* Replaces EMGrid.__init__ (fdtd.py:93-113) and the set-up part of
+ * simulate() (fdtd.py:209-255). */
+typedef struct {
+  int32_t nx, ny;
+  double dx;
+  double dt;            /* <= 0 selects 0.99 dx/(c sqrt 2) (fdtd.py:214) */
+  int32_t boundary;     /* ABSORBING, PERIODIC or REFLECTING              */
+  int32_t pml_layers;
+  int32_t device;
+} jxf_grid2d_desc;
+
+int jxf_grid2d_create(const jxf_grid2d_desc* desc, jxf_grid2d** out);
+int jxf_grid2d_destroy(jxf_grid2d* g);
+/* Line sources, replaces fdtd.py:257-262: Ez[:, y] += amp * wave[w][n]. */
+int jxf_grid2d_set_sources(jxf_grid2d* g, int32_t n, const int32_t* y,
+                           const float* amplitude, const int32_t* wave_id);
+int jxf_grid2d_set_waveforms(jxf_grid2d* g, int32_t n_waves, int64_t n_samples,
+                             const float* samples);
+/* Conductors, replaces _build_conductor_mask (fdtd.py:144-157): row y is
+ * PEC except x in [gap_start, gap_end); gap_start < 0 means a solid wall. */
+int jxf_grid2d_set_walls(jxf_grid2d* g, int32_t n, const int32_t* y,
+                         const int32_t* gap_start, const int32_t* gap_end);
+/* Replaces the scan over fdtd.py:304-364. */
+int jxf_grid2d_step(jxf_grid2d* g, int32_t n_steps, void* stream);
+int jxf_grid2d_reset(jxf_grid2d* g, void* stream);
+int jxf_grid2d_field_ptr(jxf_grid2d* g, int32_t comp, float** out);
+int jxf_grid2d_get_field(jxf_grid2d* g, int32_t comp, float* dst, int32_t dst_is_host,
+                         void* stream);
+int jxf_grid2d_set_field(jxf_grid2d* g, int32_t comp, const float* src,
+                         int32_t src_is_host, void* stream);
+/* Copy Ez, Hx, Hy into dst (device, 3*nx*ny floats): one EMFieldHistory
+ * frame (fdtd.py:359-386). */
+int jxf_grid2d_snapshot(jxf_grid2d* g, float* dst, void* stream);
+int jxf_grid2d_check_error(jxf_grid2d* g, void* stream);
+
+/* ------------------------------------------------------------------ misc */
+const char* jxf_last_error(void);
+/* Library version (major*10000 + minor*100 + patch). */
+int jxf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JAXPHYS_FDTD_H */

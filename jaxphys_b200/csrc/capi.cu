@@ -1,0 +1,1241 @@
+// C ABI of the FDTD engine: handle management, coefficient tables, TMA
+// descriptors, launch selection and the step loops.  Declarations and the
+// reference interface each entry point replaces: include/jaxphys_fdtd.h.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/jaxphys_fdtd.h"
+#include "fdtd2d_kernels.cuh"
+#include "fdtd3d_kernels.cuh"
+
+using namespace jxf;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      return fail(_e == cudaErrorMemoryAllocation ? JXF_ERR_OOM : JXF_ERR_CUDA,          \
+                  "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__,      \
+                  __LINE__);                                                             \
+  } while (0)
+
+#define TRY(expr)            \
+  do {                       \
+    int _rc = (expr);        \
+    if (_rc != JXF_OK) return _rc; \
+  } while (0)
+
+namespace {
+
+// physical constants, jaxphys src/neurosim/em/fdtd3d.py:36-38
+constexpr double kC0 = 299792458.0;
+constexpr double kPi = 3.14159265358979323846;
+const double kMu0 = 4.0e-7 * kPi;
+const double kEps0 = 1.0 / (kMu0 * kC0 * kC0);
+
+// Make `dev` current for the duration of a call, restoring the caller's.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = (cudaSetDevice(dev) == cudaSuccess);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+template <class T>
+int dmalloc(T** p, size_t count, int64_t* tally) {
+  *p = nullptr;
+  if (count == 0) return JXF_OK;
+  CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T)));
+  *tally += (int64_t)(count * sizeof(T));
+  return JXF_OK;
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+template <class T>
+int upload(T** p, const std::vector<T>& v, int64_t* tally) {
+  dfree(*p);
+  TRY(dmalloc(p, v.size(), tally));
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return JXF_OK;
+}
+
+// Reference PML conductivity profile, fdtd3d.py:149-157 / fdtd.py:173-189:
+// sigma_max*((n_pml-i)/n_pml)^3 at i and n-1-i, later writes winning.
+std::vector<double> pml_sigma(int n, int n_pml, double dx) {
+  std::vector<double> s(n, 0.0);
+  if (n_pml <= 0) return s;
+  const double sigma_max = 0.8 * 4.0 / (dx * 1.0);
+  for (int i = 0; i < n_pml; ++i) {
+    const double r = double(n_pml - i) / double(n_pml);
+    const double val = sigma_max * r * r * r;
+    if (i >= 0 && i < n) s[i] = val;
+    if (n - 1 - i >= 0 && n - 1 - i < n) s[n - 1 - i] = val;
+  }
+  return s;
+}
+
+// Separable factor of exp(-sigma_avg dt/eps0) with sigma_avg = mean over `dims`
+// axes (fdtd3d.py:221,363: dims=3; fdtd.py:242,344: dims=2).
+std::vector<float> damping_table(int n, int n_pml, double dx, double dt, int dims) {
+  std::vector<double> s = pml_sigma(n, n_pml, dx);
+  std::vector<float> d(n);
+  for (int i = 0; i < n; ++i) d[i] = (float)std::exp(-s[i] * dt / (kEps0 * dims));
+  return d;
+}
+
+// CPML 1D tables (extension).  Depth rho in [0,1] from the nearest face,
+// mirror-symmetric about (n-1)/2; sigma = sigma_max rho^m with
+// sigma_max = -(m+1) ln R0 / (2 eta0 n_pml dx); kappa = 1 + (kappa_max-1) rho^m;
+// alpha = alpha_max (1-rho); b = exp(-(sigma/kappa + alpha) dt/eps0);
+// c = sigma (b-1) / (sigma kappa + kappa^2 alpha).
+void cpml_tables(int n, int n_pml, double dx, double dt, double m, double r0, double kmax,
+                 double amax, std::vector<float> out[TAB_COUNT]) {
+  const double eta0 = std::sqrt(kMu0 / kEps0);
+  const double smax = n_pml > 0 ? -(m + 1.0) * std::log(r0) / (2.0 * eta0 * n_pml * dx) : 0.0;
+  for (int t = 0; t < TAB_COUNT; ++t) out[t].assign(n, 0.0f);
+  for (int half = 0; half < 2; ++half) {
+    for (int i = 0; i < n; ++i) {
+      const double x = i + 0.5 * half;
+      double rho = 0.0;
+      if (n_pml > 0) {
+        const double lo = (n_pml - x) / n_pml;
+        const double hi = (x - (n - 1 - n_pml)) / n_pml;
+        rho = std::min(1.0, std::max(0.0, std::max(lo, hi)));
+      }
+      const double pm = std::pow(rho, m);
+      const double sigma = smax * pm;
+      const double kappa = 1.0 + (kmax - 1.0) * pm;
+      const double alpha = rho > 0.0 ? amax * (1.0 - rho) : 0.0;
+      const double b = std::exp(-(sigma / kappa + alpha) * dt / kEps0);
+      const double den = sigma * kappa + kappa * kappa * alpha;
+      const double c = sigma > 0.0 ? sigma * (b - 1.0) / (den > 0.0 ? den : 1.0) : 0.0;
+      const int base = half ? TAB_BH : TAB_BE;
+      out[base + 0][i] = (float)b;
+      out[base + 1][i] = (float)c;
+      out[base + 2][i] = (float)(1.0 / kappa);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// TMA descriptors
+// ---------------------------------------------------------------------------
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int get_encoder() {
+  if (g_encode) return JXF_OK;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (q != cudaDriverEntryPointSuccess || fn == nullptr)
+    return fail(JXF_ERR_CUDA, "cuTensorMapEncodeTiled not available from the driver");
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return JXF_OK;
+}
+
+// Tiled map over a float32 (nx, ny, nz) array, box {bz, by, 1}.
+int encode_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, int bz, int by) {
+  TRY(get_encoder());
+  cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
+  cuuint64_t strides[2] = {(cuuint64_t)nz * 4, (cuuint64_t)nz * ny * 4};
+  cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(JXF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return JXF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// TMA kernel registry
+// ---------------------------------------------------------------------------
+
+using TmaKernel = void (*)(const Step3D, const Maps3D);
+
+struct TmaConfig {
+  int tz, ty, ry, stages;
+  int threads;
+  size_t smem[2];     // [mode: 0 absorb, 1 cpml]
+  TmaKernel k[2][2];  // [mode: 0 absorb, 1 cpml][cbarr]
+};
+
+template <int TZ, int TY, int RY, int ST>
+TmaConfig make_cfg() {
+  TmaConfig c;
+  c.tz = TZ;
+  c.ty = TY;
+  c.ry = RY;
+  c.stages = ST;
+  c.threads = TZ * (TY / RY);
+  c.smem[0] = TmaLayout<TZ, TY, RY, ST, true, false>::SMEM_BYTES;
+  c.smem[1] = TmaLayout<TZ, TY, RY, ST, true, true>::SMEM_BYTES;
+  c.k[0][0] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, false>;
+  c.k[0][1] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, true>;
+  c.k[1][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false>;
+  c.k[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true>;
+  return c;
+}
+
+const std::vector<TmaConfig>& tma_configs() {
+  static const std::vector<TmaConfig> cfgs = {
+      make_cfg<32, 8, 1, 4>(),  make_cfg<32, 16, 2, 4>(), make_cfg<64, 8, 2, 3>(),
+      make_cfg<32, 16, 4, 4>(), make_cfg<64, 16, 4, 3>(),
+  };
+  return cfgs;
+}
+
+// autotune results: (nx, ny, nz, mode, cbarr) -> (cfg index, x_chunk)
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// 3D handle
+// ---------------------------------------------------------------------------
+
+struct jxf_grid3d {
+  jxf_grid3d_desc d{};
+  int mode = MODE_ABSORB;   // kernel mode: ABSORB (also PEC with unit tables), PERIODIC, CPML
+  int path = JXF_PATH_GENERIC;
+  double dt = 0, coef_h = 0, coef_e = 0;
+  long long n = 0;
+  int64_t bytes = 0;
+  float* f[2][6] = {};
+  float* cb = nullptr;
+  float* damp[3] = {};
+  float* tab[3][TAB_COUNT] = {};
+  float* psi[2][PSI_COUNT] = {};
+  int L[3] = {0, 0, 0}, P[3] = {-1, -1, -1};
+  int cur = 0;
+  long long step = 0;
+  // sources (host copies kept to rebuild per-block lists)
+  std::vector<long long> src_cell;
+  std::vector<int> src_comp, src_wave;
+  std::vector<float> src_amp;
+  SrcCell* d_cells = nullptr;
+  SrcTerm* d_terms = nullptr;
+  int n_cells = 0;
+  SrcEntry* d_entries = nullptr;
+  int* d_blk_ptr = nullptr;
+  int n_blocks_built = -1;
+  int built_cfg = -1, built_chunk = -1;
+  float* d_wave = nullptr;
+  int n_waves = 0;
+  long long wave_len = 0;
+  // probes
+  long long* d_probe_cell = nullptr;
+  int* d_probe_comp = nullptr;
+  int n_probes = 0;
+  int* d_err = nullptr;
+  int* d_count = nullptr;
+  // TMA selection
+  int cfg = -1, x_chunk = 0;
+  bool maps_ok = false;
+  int maps_cfg = -1;  // config whose box shapes the maps were encoded with
+  Maps3D maps[2];     // input set 0 / 1
+};
+
+namespace {
+
+int cells_ok(const jxf_grid3d* g, long long cell) { return cell >= 0 && cell < g->n; }
+
+int build_generic_sources(jxf_grid3d* g) {
+  // group by (cell, comp) in order of first appearance; terms in list order
+  std::map<std::pair<long long, int>, std::vector<int>> groups;
+  std::vector<std::pair<long long, int>> order;
+  for (size_t i = 0; i < g->src_cell.size(); ++i) {
+    auto key = std::make_pair(g->src_cell[i], g->src_comp[i]);
+    auto it = groups.find(key);
+    if (it == groups.end()) {
+      order.push_back(key);
+      groups[key] = {(int)i};
+    } else {
+      it->second.push_back((int)i);
+    }
+  }
+  std::vector<SrcCell> cells;
+  std::vector<SrcTerm> terms;
+  for (auto& key : order) {
+    SrcCell c{};
+    c.cell = key.first;
+    c.comp = key.second;
+    c.first = (int)terms.size();
+    for (int i : groups[key]) terms.push_back(SrcTerm{g->src_amp[i], g->src_wave[i]});
+    c.count = (int)terms.size() - c.first;
+    cells.push_back(c);
+  }
+  g->n_cells = (int)cells.size();
+  TRY(upload(&g->d_cells, cells, &g->bytes));
+  TRY(upload(&g->d_terms, terms, &g->bytes));
+  return JXF_OK;
+}
+
+// Per-block source lists for the TMA kernel: CSR over blocks, entries sorted
+// by plane, list order kept inside a plane (stable sort).
+int build_tma_sources(jxf_grid3d* g) {
+  const TmaConfig& c = tma_configs()[g->cfg];
+  const int ny = g->d.ny, nz = g->d.nz, nx = g->d.nx;
+  const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
+  const int nch = (nx + g->x_chunk - 1) / g->x_chunk;
+  const int nblk = ntz * nty * nch;
+  std::vector<std::pair<int, int>> keyed;  // (block, source index)
+  for (size_t i = 0; i < g->src_cell.size(); ++i) {
+    const long long cell = g->src_cell[i];
+    const int z = (int)(cell % nz);
+    const int y = (int)((cell / nz) % ny);
+    const int x = (int)(cell / ((long long)nz * ny));
+    const int b = ((x / g->x_chunk) * nty + y / c.ty) * ntz + z / c.tz;
+    keyed.push_back({b, (int)i});
+  }
+  std::stable_sort(keyed.begin(), keyed.end(), [&](const auto& u, const auto& v) {
+    if (u.first != v.first) return u.first < v.first;
+    const long long xu = g->src_cell[u.second] / ((long long)nz * ny);
+    const long long xv = g->src_cell[v.second] / ((long long)nz * ny);
+    return xu < xv;
+  });
+  std::vector<int> ptr(nblk + 1, 0);
+  std::vector<SrcEntry> ents;
+  for (auto& kv : keyed) {
+    const int i = kv.second;
+    const long long cell = g->src_cell[i];
+    const int z = (int)(cell % nz);
+    const int y = (int)((cell / nz) % ny);
+    const int x = (int)(cell / ((long long)nz * ny));
+    SrcEntry e{};
+    e.x = x;
+    e.off = (y % c.ty) * c.tz + (z % c.tz);
+    e.comp = g->src_comp[i];
+    e.wave = g->src_wave[i];
+    e.amp = g->src_amp[i];
+    ents.push_back(e);
+    ptr[kv.first + 1]++;
+  }
+  for (int b = 0; b < nblk; ++b) ptr[b + 1] += ptr[b];
+  TRY(upload(&g->d_entries, ents, &g->bytes));
+  TRY(upload(&g->d_blk_ptr, ptr, &g->bytes));
+  g->built_cfg = g->cfg;
+  g->built_chunk = g->x_chunk;
+  return JXF_OK;
+}
+
+int encode_maps(jxf_grid3d* g) {
+  const TmaConfig& c = tma_configs()[g->cfg];
+  const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
+  for (int s = 0; s < 2; ++s) {
+    for (int k = 0; k < 3; ++k) {
+      TRY(encode_map(&g->maps[s].e[k], g->f[s][k], nx, ny, nz, c.tz + 8, c.ty + 2));
+      TRY(encode_map(&g->maps[s].h[k], g->f[s][3 + k], nx, ny, nz, c.tz + 4, c.ty + 1));
+    }
+    if (g->cb) {
+      TRY(encode_map(&g->maps[s].cb, g->cb, nx, ny, nz, c.tz, c.ty));
+    } else {
+      g->maps[s].cb = g->maps[s].e[0];  // unused
+    }
+  }
+  g->maps_ok = true;
+  g->maps_cfg = g->cfg;
+  return JXF_OK;
+}
+
+// Bound on every device-side wait: 2 s, or JXF_WAIT_LIMIT_MS.
+unsigned long long wait_limit_ns() {
+  static unsigned long long v = [] {
+    const char* e = std::getenv("JXF_WAIT_LIMIT_MS");
+    long long ms = e ? std::atoll(e) : 2000;
+    if (ms < 1) ms = 1;
+    return (unsigned long long)ms * 1000000ull;
+  }();
+  return v;
+}
+
+Step3D base_params(jxf_grid3d* g) {
+  Step3D p{};
+  p.nx = g->d.nx;
+  p.ny = g->d.ny;
+  p.nz = g->d.nz;
+  p.a = (float)g->coef_h;
+  p.cb_const = (float)g->coef_e;
+  p.cb = g->cb;
+  for (int k = 0; k < 3; ++k) p.damp[k] = g->damp[k];
+  for (int ax = 0; ax < 3; ++ax) {
+    for (int t = 0; t < TAB_COUNT; ++t) p.pml.tab[ax][t] = g->tab[ax][t];
+    p.pml.L[ax] = g->L[ax];
+    p.pml.P[ax] = g->P[ax];
+  }
+  p.wave = g->d_wave;
+  p.wave_len = g->wave_len;
+  p.n_probes = g->n_probes;
+  p.probe_cell = g->d_probe_cell;
+  p.probe_comp = g->d_probe_comp;
+  p.err = g->d_err;
+  p.wait_ns = wait_limit_ns();
+  return p;
+}
+
+void set_io(jxf_grid3d* g, Step3D& p, int in_set, int out_set) {
+  for (int k = 0; k < 6; ++k) {
+    p.in[k] = g->f[in_set][k];
+    p.out[k] = g->f[out_set][k];
+  }
+  for (int k = 0; k < PSI_COUNT; ++k) {
+    p.pml.in[k] = g->psi[in_set][k];
+    p.pml.out[k] = g->psi[out_set][k];
+  }
+}
+
+int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStream_t st) {
+  // The boxes of the tensor maps must be the ones this config's kernel expects
+  // (the mbarrier transaction count is derived from them).
+  if (!g->maps_ok || g->maps_cfg != cfg)
+    return fail(JXF_ERR_INVALID, "tensor maps encoded for config %d, launching config %d",
+                g->maps_cfg, cfg);
+  const TmaConfig& c = tma_configs()[cfg];
+  const int mi = g->mode == MODE_CPML ? 1 : 0;
+  TmaKernel k = c.k[mi][g->cb ? 1 : 0];
+  const size_t smem = c.smem[mi];
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  p.x_chunk = chunk;
+  p.ntiles_z = (g->d.nz + c.tz - 1) / c.tz;
+  p.ntiles_y = (g->d.ny + c.ty - 1) / c.ty;
+  dim3 grid(p.ntiles_z, p.ntiles_y, (g->d.nx + chunk - 1) / chunk);
+  k<<<grid, c.threads, smem, st>>>(p, g->maps[in_set]);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+int heuristic_tune(jxf_grid3d* g) {
+  // Small grids: smaller tiles and chunks keep >= 2 waves of blocks.
+  const long long cells = g->n;
+  g->cfg = 0;
+  g->x_chunk = cells >= (1LL << 24) ? 64 : (cells >= (1LL << 21) ? 16 : 8);
+  return JXF_OK;
+}
+
+// Time every (config, chunk) on A -> B launches (the state in A and the step
+// counter are untouched, probes off) and keep the fastest.
+int autotune(jxf_grid3d* g, cudaStream_t st) {
+  const auto key = std::make_tuple(g->d.nx, g->d.ny, g->d.nz, g->mode, g->cb ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      g->cfg = it->second.first;
+      g->x_chunk = it->second.second;
+      return JXF_OK;
+    }
+  }
+  const char* env = std::getenv("JXF_AUTOTUNE");
+  const bool enabled = !(env && env[0] == '0');
+  if (!enabled || g->n < (1LL << 18)) {
+    TRY(heuristic_tune(g));
+  } else {
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bc = 0, bk = 8;
+    const int chunks[] = {8, 16, 32, 64};
+    for (int ci = 0; ci < (int)tma_configs().size(); ++ci) {
+      for (int ch : chunks) {
+        if (ch > g->d.nx && ch != 8) continue;
+        g->cfg = ci;
+        g->x_chunk = ch;
+        TRY(encode_maps(g));
+        Step3D p = base_params(g);
+        set_io(g, p, g->cur, 1 - g->cur);
+        p.blk_src_ptr = nullptr;
+        p.probe_out = nullptr;
+        p.step = 0;
+        p.err = g->d_err;
+        TRY(launch_tma(g, ci, ch, p, g->cur, st));
+        CUDA_TRY(cudaEventRecord(e0, st));
+        const int reps = g->n >= (1LL << 25) ? 3 : 10;
+        for (int r = 0; r < reps; ++r) TRY(launch_tma(g, ci, ch, p, g->cur, st));
+        CUDA_TRY(cudaEventRecord(e1, st));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+          best = ms;
+          bc = ci;
+          bk = ch;
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g->cfg = bc;
+    g->x_chunk = bk;
+    g->maps_ok = false;  // maps hold the boxes of the last trial, not of the winner
+    g->built_cfg = -1;
+    // The trials wrote only the idle buffer set, which the next real step
+    // overwrites before anything reads it.
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = {g->cfg, g->x_chunk};
+  return JXF_OK;
+}
+
+int ensure_tma_ready(jxf_grid3d* g, cudaStream_t st) {
+  if (g->cfg < 0) TRY(autotune(g, st));
+  if (!g->maps_ok) TRY(encode_maps(g));
+  if (!g->src_cell.empty() && (g->built_cfg != g->cfg || g->built_chunk != g->x_chunk))
+    TRY(build_tma_sources(g));
+  return JXF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* jxf_last_error(void) { return g_last_error.c_str(); }
+
+int jxf_version(void) { return 100; }
+
+int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out) {
+  if (!desc || !out) return fail(JXF_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const jxf_grid3d_desc d = *desc;
+  if (d.nx < 2 || d.ny < 2 || d.nz < 2)
+    return fail(JXF_ERR_INVALID, "grid must be at least 2 cells per axis, got %dx%dx%d", d.nx, d.ny,
+                d.nz);
+  if ((long long)d.nx * d.ny * d.nz > (1LL << 36))
+    return fail(JXF_ERR_INVALID, "grid too large");
+  if (!(d.dx > 0)) return fail(JXF_ERR_INVALID, "dx must be positive");
+  if (d.pml_layers < 0) return fail(JXF_ERR_INVALID, "pml_layers must be >= 0");
+  if (d.boundary != JXF_BND_ABSORBING && d.boundary != JXF_BND_PERIODIC &&
+      d.boundary != JXF_BND_PEC && d.boundary != JXF_BND_CPML)
+    return fail(JXF_ERR_INVALID, "unsupported 3D boundary %d", d.boundary);
+  if (d.boundary == JXF_BND_CPML && !(d.cpml_r0 > 0 && d.cpml_r0 < 1))
+    return fail(JXF_ERR_INVALID, "cpml_r0 must be in (0, 1)");
+  DeviceGuard dg(d.device);
+  if (!dg.ok) return fail(JXF_ERR_CUDA, "cannot select device %d", d.device);
+
+  jxf_grid3d* g = new jxf_grid3d();
+  g->d = d;
+  g->n = (long long)d.nx * d.ny * d.nz;
+  g->dt = d.dt > 0 ? d.dt : 0.99 * d.dx / (kC0 * std::sqrt(3.0));  // fdtd3d.py:190-192
+  g->coef_h = g->dt / (kMu0 * d.dx);                                 // fdtd3d.py:223
+  g->coef_e = g->dt / (kEps0 * d.dx);                                // fdtd3d.py:224
+  g->mode = d.boundary == JXF_BND_PERIODIC ? MODE_PERIODIC
+            : d.boundary == JXF_BND_CPML   ? MODE_CPML
+                                           : MODE_ABSORB;
+  const bool tma_ok = (d.nz % 4 == 0) && g->mode != MODE_PERIODIC;
+  if (d.path == JXF_PATH_TMA && !tma_ok) {
+    delete g;
+    return fail(JXF_ERR_INVALID, "TMA path needs nz %% 4 == 0 and a non-periodic boundary");
+  }
+  g->path = (d.path == JXF_PATH_GENERIC || !tma_ok) ? JXF_PATH_GENERIC : JXF_PATH_TMA;
+
+  auto cleanup_fail = [&](int rc) {
+    jxf_grid3d_destroy(g);
+    return rc;
+  };
+  int rc;
+  for (int s = 0; s < 2; ++s)
+    for (int k = 0; k < 6; ++k) {
+      if (s == 1 && g->path == JXF_PATH_GENERIC) break;
+      if ((rc = dmalloc(&g->f[s][k], (size_t)g->n, &g->bytes)) != JXF_OK) return cleanup_fail(rc);
+      cudaMemset(g->f[s][k], 0, (size_t)g->n * 4);
+    }
+  if (g->path == JXF_PATH_GENERIC)
+    for (int k = 0; k < 6; ++k) g->f[1][k] = g->f[0][k];
+
+  const int dims[3] = {d.nx, d.ny, d.nz};
+  // damping tables (ones for PEC / CPML / PERIODIC)
+  for (int ax = 0; ax < 3; ++ax) {
+    std::vector<float> t = (d.boundary == JXF_BND_ABSORBING)
+                               ? damping_table(dims[ax], d.pml_layers, d.dx, g->dt, 3)
+                               : std::vector<float>(dims[ax], 1.0f);
+    if ((rc = upload(&g->damp[ax], t, &g->bytes)) != JXF_OK) return cleanup_fail(rc);
+  }
+  if (g->mode == MODE_CPML) {
+    const double m = d.cpml_order > 0 ? d.cpml_order : 3.0;
+    const double kmax = d.cpml_kappa_max >= 1.0 ? d.cpml_kappa_max : 1.0;
+    for (int ax = 0; ax < 3; ++ax) {
+      std::vector<float> t[TAB_COUNT];
+      cpml_tables(dims[ax], d.pml_layers, d.dx, g->dt, m, d.cpml_r0, kmax, d.cpml_alpha_max, t);
+      for (int k = 0; k < TAB_COUNT; ++k)
+        if ((rc = upload(&g->tab[ax][k], t[k], &g->bytes)) != JXF_OK) return cleanup_fail(rc);
+      const int P = d.pml_layers + 1;
+      if (2 * P >= dims[ax]) {
+        g->P[ax] = -1;
+        g->L[ax] = dims[ax];
+      } else {
+        g->P[ax] = P;
+        g->L[ax] = 2 * P;
+      }
+    }
+    const size_t sz_x = (size_t)g->L[0] * d.ny * d.nz;
+    const size_t sz_y = (size_t)d.nx * g->L[1] * d.nz;
+    const size_t sz_z = (size_t)d.nx * d.ny * g->L[2];
+    const int axis_of[PSI_COUNT] = {1, 2, 2, 0, 0, 1, 1, 2, 2, 0, 0, 1};
+    for (int s = 0; s < 2; ++s)
+      for (int k = 0; k < PSI_COUNT; ++k) {
+        if (s == 1 && g->path == JXF_PATH_GENERIC) {
+          g->psi[1][k] = g->psi[0][k];
+          continue;
+        }
+        const size_t sz = axis_of[k] == 0 ? sz_x : (axis_of[k] == 1 ? sz_y : sz_z);
+        if ((rc = dmalloc(&g->psi[s][k], sz, &g->bytes)) != JXF_OK) return cleanup_fail(rc);
+        cudaMemset(g->psi[s][k], 0, sz * 4);
+      }
+  } else {
+    // tables are dereferenced only in CPML mode; keep valid pointers anyway
+    for (int ax = 0; ax < 3; ++ax)
+      for (int k = 0; k < TAB_COUNT; ++k) g->tab[ax][k] = g->damp[ax];
+  }
+  if ((rc = dmalloc(&g->d_err, 4, &g->bytes)) != JXF_OK) return cleanup_fail(rc);
+  if ((rc = dmalloc(&g->d_count, 1, &g->bytes)) != JXF_OK) return cleanup_fail(rc);
+  cudaMemset(g->d_err, 0, 16);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess)
+    return cleanup_fail(fail(JXF_ERR_CUDA, "initialisation failed: %s", cudaGetErrorString(e)));
+  *out = g;
+  return JXF_OK;
+}
+
+int jxf_grid3d_destroy(jxf_grid3d* g) {
+  if (!g) return JXF_OK;
+  DeviceGuard dg(g->d.device);
+  const bool shared_f = g->path == JXF_PATH_GENERIC;
+  for (int s = 0; s < 2; ++s)
+    for (int k = 0; k < 6; ++k) {
+      if (s == 1 && shared_f) break;
+      dfree(g->f[s][k]);
+    }
+  const bool cpml = g->mode == MODE_CPML;
+  for (int s = 0; s < 2; ++s)
+    for (int k = 0; k < PSI_COUNT; ++k) {
+      if (s == 1 && shared_f) break;
+      dfree(g->psi[s][k]);
+    }
+  if (cpml)
+    for (int ax = 0; ax < 3; ++ax)
+      for (int k = 0; k < TAB_COUNT; ++k) dfree(g->tab[ax][k]);
+  for (int ax = 0; ax < 3; ++ax) dfree(g->damp[ax]);
+  dfree(g->cb);
+  dfree(g->d_cells);
+  dfree(g->d_terms);
+  dfree(g->d_entries);
+  dfree(g->d_blk_ptr);
+  dfree(g->d_wave);
+  dfree(g->d_probe_cell);
+  dfree(g->d_probe_comp);
+  dfree(g->d_err);
+  dfree(g->d_count);
+  delete g;
+  return JXF_OK;
+}
+
+int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
+  if (!g || !out) return fail(JXF_ERR_INVALID, "null argument");
+  out->dt = g->dt;
+  out->coef_h = g->coef_h;
+  out->coef_e = g->coef_e;
+  out->step = g->step;
+  out->path = g->path;
+  if (g->path == JXF_PATH_TMA && g->cfg >= 0) {
+    const TmaConfig& c = tma_configs()[g->cfg];
+    out->tile_z = c.tz;
+    out->tile_y = c.ty;
+    out->rows_per_thread = c.ry;
+    out->stages = c.stages;
+    out->x_chunk = g->x_chunk;
+  } else {
+    out->tile_z = out->tile_y = out->rows_per_thread = out->stages = out->x_chunk = 0;
+  }
+  out->device_bytes = g->bytes;
+  return JXF_OK;
+}
+
+// Fix the TMA launch shape (cfg index into the registry, planes per block);
+// cfg < 0 re-enables autotuning.
+int jxf_grid3d_set_launch(jxf_grid3d* g, int32_t cfg, int32_t x_chunk) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (g->path != JXF_PATH_TMA) return fail(JXF_ERR_INVALID, "grid does not use the TMA path");
+  if (cfg >= (int)tma_configs().size()) return fail(JXF_ERR_INVALID, "cfg out of range");
+  if (cfg >= 0 && x_chunk < 1) return fail(JXF_ERR_INVALID, "x_chunk must be >= 1");
+  g->cfg = cfg;
+  g->x_chunk = x_chunk;
+  g->maps_ok = false;
+  g->built_cfg = -1;
+  return JXF_OK;
+}
+
+int jxf_num_tma_configs(void) { return (int)tma_configs().size(); }
+
+static __global__ void k_cb_from_eps(const float* eps, float* cb, float coef, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    cb[i] = __fdiv_rn(coef, eps[i]);
+}
+
+int jxf_grid3d_set_eps_host(jxf_grid3d* g, const double* eps_r) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(g->d.device);
+  if (!eps_r) {
+    dfree(g->cb);
+    g->maps_ok = false;
+    return JXF_OK;
+  }
+  std::vector<float> cb((size_t)g->n);
+  for (long long i = 0; i < g->n; ++i) {
+    if (!(eps_r[i] > 0) || !std::isfinite(eps_r[i]))
+      return fail(JXF_ERR_INVALID, "eps_r must be finite and positive (cell %lld)", i);
+    cb[i] = (float)(g->coef_e / eps_r[i]);  // fdtd3d.py:299 (dt_eps_dx / eps_r), FP64 then round
+  }
+  TRY(upload(&g->cb, cb, &g->bytes));
+  g->maps_ok = false;
+  return JXF_OK;
+}
+
+int jxf_grid3d_set_eps_device(jxf_grid3d* g, const float* eps_r, void* stream) {
+  if (!g || !eps_r) return fail(JXF_ERR_INVALID, "null argument");
+  DeviceGuard dg(g->d.device);
+  if (!g->cb) {
+    TRY(dmalloc(&g->cb, (size_t)g->n, &g->bytes));
+  }
+  k_cb_from_eps<<<592, 256, 0, (cudaStream_t)stream>>>(eps_r, g->cb, (float)g->coef_e, g->n);
+  CUDA_TRY(cudaGetLastError());
+  g->maps_ok = false;
+  return JXF_OK;
+}
+
+int jxf_grid3d_set_sources(jxf_grid3d* g, int32_t n, const int64_t* cell, const int32_t* comp,
+                           const float* amplitude, const int32_t* wave_id) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n < 0 || (n > 0 && (!cell || !comp || !amplitude || !wave_id)))
+    return fail(JXF_ERR_INVALID, "bad source arrays");
+  DeviceGuard dg(g->d.device);
+  for (int i = 0; i < n; ++i) {
+    if (!cells_ok(g, cell[i])) return fail(JXF_ERR_INVALID, "source %d: cell out of grid", i);
+    if (comp[i] < 0 || comp[i] > 2) return fail(JXF_ERR_INVALID, "source %d: comp must be 0..2", i);
+    if (wave_id[i] < 0) return fail(JXF_ERR_INVALID, "source %d: negative wave id", i);
+  }
+  g->src_cell.assign(cell, cell + n);
+  g->src_comp.assign(comp, comp + n);
+  g->src_amp.assign(amplitude, amplitude + n);
+  g->src_wave.assign(wave_id, wave_id + n);
+  TRY(build_generic_sources(g));
+  g->built_cfg = -1;
+  return JXF_OK;
+}
+
+int jxf_grid3d_set_waveforms(jxf_grid3d* g, int32_t n_waves, int64_t n_samples,
+                             const float* samples) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n_waves < 0 || n_samples < 0 || (n_waves * n_samples > 0 && !samples))
+    return fail(JXF_ERR_INVALID, "bad waveform table");
+  DeviceGuard dg(g->d.device);
+  std::vector<float> v(samples, samples + (size_t)n_waves * n_samples);
+  TRY(upload(&g->d_wave, v, &g->bytes));
+  g->n_waves = n_waves;
+  g->wave_len = n_samples;
+  return JXF_OK;
+}
+
+int jxf_grid3d_set_probes(jxf_grid3d* g, int32_t n, const int64_t* cell, const int32_t* comp) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n < 0 || (n > 0 && (!cell || !comp))) return fail(JXF_ERR_INVALID, "bad probe arrays");
+  DeviceGuard dg(g->d.device);
+  for (int i = 0; i < n; ++i) {
+    if (!cells_ok(g, cell[i])) return fail(JXF_ERR_INVALID, "probe %d: cell out of grid", i);
+    if (comp[i] < 0 || comp[i] > 5) return fail(JXF_ERR_INVALID, "probe %d: comp must be 0..5", i);
+  }
+  std::vector<long long> c(cell, cell + n);
+  std::vector<int> k(comp, comp + n);
+  TRY(upload(&g->d_probe_cell, c, &g->bytes));
+  TRY(upload(&g->d_probe_comp, k, &g->bytes));
+  g->n_probes = n;
+  return JXF_OK;
+}
+
+static int gather_probes(jxf_grid3d* g, int set, float* out, cudaStream_t st) {
+  if (g->n_probes == 0 || !out) return JXF_OK;
+  FieldPtrs6 fp;
+  for (int k = 0; k < 6; ++k) fp.f[k] = g->f[set][k];
+  k_probe_gather<<<(g->n_probes + 127) / 128, 128, 0, st>>>(fp, g->d_probe_cell, g->d_probe_comp,
+                                                           g->n_probes, out);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n_steps < 0) return fail(JXF_ERR_INVALID, "n_steps must be >= 0");
+  if (n_steps == 0) return JXF_OK;
+  if (!g->src_cell.empty()) {
+    int max_w = 0;
+    for (int w : g->src_wave) max_w = std::max(max_w, w);
+    if (max_w >= g->n_waves)
+      return fail(JXF_ERR_INVALID, "source wave id %d has no waveform row", max_w);
+    if (g->step + n_steps > g->wave_len)
+      return fail(JXF_ERR_INVALID, "waveform table covers %lld steps, need %lld", g->wave_len,
+                  g->step + n_steps);
+  }
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  Step3D p = base_params(g);
+  const int np = g->n_probes;
+  if (g->path == JXF_PATH_TMA) {
+    TRY(ensure_tma_ready(g, st));
+    p.blk_src_ptr = g->src_cell.empty() ? nullptr : g->d_blk_ptr;
+    p.src = g->d_entries;
+    for (int k = 0; k < n_steps; ++k) {
+      set_io(g, p, g->cur, 1 - g->cur);
+      p.step = g->step;
+      p.probe_out = (probe_out && np > 0 && k >= 1) ? probe_out + (size_t)(k - 1) * np : nullptr;
+      TRY(launch_tma(g, g->cfg, g->x_chunk, p, g->cur, st));
+      g->cur ^= 1;
+      g->step++;
+    }
+    if (probe_out && np > 0) TRY(gather_probes(g, g->cur, probe_out + (size_t)(n_steps - 1) * np, st));
+  } else {
+    const int threads = 256;
+    const long long blocks_needed = (g->n + threads - 1) / threads;
+    const int blocks = (int)std::min<long long>(blocks_needed, 148LL * 16);
+    for (int k = 0; k < n_steps; ++k) {
+      set_io(g, p, 0, 0);
+      p.step = g->step;
+      switch (g->mode) {
+        case MODE_PERIODIC:
+          jxf::k3d_generic_h<MODE_PERIODIC><<<blocks, threads, 0, st>>>(p);
+          jxf::k3d_generic_e<MODE_PERIODIC><<<blocks, threads, 0, st>>>(p);
+          break;
+        case MODE_CPML:
+          jxf::k3d_generic_h<MODE_CPML><<<blocks, threads, 0, st>>>(p);
+          jxf::k3d_generic_e<MODE_CPML><<<blocks, threads, 0, st>>>(p);
+          break;
+        default:
+          jxf::k3d_generic_h<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+          jxf::k3d_generic_e<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+          break;
+      }
+      CUDA_TRY(cudaGetLastError());
+      if (g->n_cells > 0) {
+        k3d_sources<<<(g->n_cells + 127) / 128, 128, 0, st>>>(
+            g->f[0][0], g->f[0][1], g->f[0][2], g->d_cells, g->n_cells, g->d_terms, g->d_wave,
+            g->wave_len, g->step);
+        CUDA_TRY(cudaGetLastError());
+      }
+      if (probe_out && np > 0) TRY(gather_probes(g, 0, probe_out + (size_t)k * np, st));
+      g->step++;
+    }
+  }
+  return JXF_OK;
+}
+
+int jxf_grid3d_reset(jxf_grid3d* g, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int sets = g->path == JXF_PATH_GENERIC ? 1 : 2;
+  for (int s = 0; s < sets; ++s) {
+    for (int k = 0; k < 6; ++k) CUDA_TRY(cudaMemsetAsync(g->f[s][k], 0, (size_t)g->n * 4, st));
+    if (g->mode == MODE_CPML) {
+      const size_t sz_x = (size_t)g->L[0] * g->d.ny * g->d.nz;
+      const size_t sz_y = (size_t)g->d.nx * g->L[1] * g->d.nz;
+      const size_t sz_z = (size_t)g->d.nx * g->d.ny * g->L[2];
+      const int axis_of[PSI_COUNT] = {1, 2, 2, 0, 0, 1, 1, 2, 2, 0, 0, 1};
+      for (int k = 0; k < PSI_COUNT; ++k) {
+        const size_t sz = axis_of[k] == 0 ? sz_x : (axis_of[k] == 1 ? sz_y : sz_z);
+        CUDA_TRY(cudaMemsetAsync(g->psi[s][k], 0, sz * 4, st));
+      }
+    }
+  }
+  g->cur = 0;
+  g->step = 0;
+  return JXF_OK;
+}
+
+int jxf_grid3d_field_ptr(jxf_grid3d* g, int32_t comp, float** out) {
+  if (!g || !out) return fail(JXF_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 5) return fail(JXF_ERR_INVALID, "comp must be 0..5");
+  *out = g->f[g->cur][comp];
+  return JXF_OK;
+}
+
+int jxf_grid3d_get_field(jxf_grid3d* g, int32_t comp, float* dst, int32_t dst_is_host,
+                         void* stream) {
+  if (!g || !dst) return fail(JXF_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 5) return fail(JXF_ERR_INVALID, "comp must be 0..5");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(dst, g->f[g->cur][comp], (size_t)g->n * 4,
+                           dst_is_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
+  if (dst_is_host) CUDA_TRY(cudaStreamSynchronize(st));
+  return JXF_OK;
+}
+
+int jxf_grid3d_set_field(jxf_grid3d* g, int32_t comp, const float* src, int32_t src_is_host,
+                         void* stream) {
+  if (!g || !src) return fail(JXF_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 5) return fail(JXF_ERR_INVALID, "comp must be 0..5");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(g->f[g->cur][comp], src, (size_t)g->n * 4,
+                           src_is_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+  if (src_is_host) CUDA_TRY(cudaStreamSynchronize(st));
+  return JXF_OK;
+}
+
+int jxf_grid3d_snapshot(jxf_grid3d* g, float* dst, void* stream) {
+  if (!g || !dst) return fail(JXF_ERR_INVALID, "null argument");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int k = 0; k < 6; ++k)
+    CUDA_TRY(cudaMemcpyAsync(dst + (size_t)k * g->n, g->f[g->cur][k], (size_t)g->n * 4,
+                             cudaMemcpyDeviceToDevice, st));
+  return JXF_OK;
+}
+
+int jxf_grid3d_check_error(jxf_grid3d* g, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int h[4] = {0, 0, 0, 0};
+  CUDA_TRY(cudaMemcpyAsync(h, g->d_err, 16, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  CUDA_TRY(cudaGetLastError());
+  if (h[0] != 0) {
+    CUDA_TRY(cudaMemsetAsync(g->d_err, 0, 16, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (h[0] & ERR_TIMEOUT_BASE)
+      return fail(JXF_ERR_TIMEOUT,
+                  "a staged copy did not arrive within the wait limit (block %d, plane index %d, "
+                  "copies issued %d)",
+                  h[1], h[2], h[3]);
+    return fail(JXF_ERR_CUDA, "device error word 0x%x", h[0]);
+  }
+  return JXF_OK;
+}
+
+static __global__ void k_count_nonfinite(const float* f, long long n, int* count) {
+  int local = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    local += !isfinite(f[i]);
+  if (local) atomicAdd(count, local);
+}
+
+int jxf_grid3d_check_finite(jxf_grid3d* g, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemsetAsync(g->d_count, 0, 4, st));
+  for (int k = 0; k < 6; ++k) k_count_nonfinite<<<592, 256, 0, st>>>(g->f[g->cur][k], g->n, g->d_count);
+  CUDA_TRY(cudaGetLastError());
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, g->d_count, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) return fail(JXF_ERR_NONFINITE, "%d non-finite field values", h);
+  return JXF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// 2D handle
+// ---------------------------------------------------------------------------
+
+struct jxf_grid2d {
+  jxf_grid2d_desc d{};
+  int mode = MODE_ABSORB;
+  double dt = 0, coef_h = 0, coef_e = 0;
+  long long n = 0;
+  int64_t bytes = 0;
+  float* f[3] = {};
+  float* damp[2] = {};
+  int n_src = 0;
+  int* d_src_y = nullptr;
+  float* d_src_amp = nullptr;
+  int* d_src_wave = nullptr;
+  std::vector<int> src_wave;
+  float* d_wave = nullptr;
+  int n_waves = 0;
+  long long wave_len = 0;
+  int n_wall = 0;
+  int* d_wall_y = nullptr;
+  int* d_wall_g0 = nullptr;
+  int* d_wall_g1 = nullptr;
+  long long step = 0;
+};
+
+extern "C" {
+
+int jxf_grid2d_create(const jxf_grid2d_desc* desc, jxf_grid2d** out) {
+  if (!desc || !out) return fail(JXF_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const jxf_grid2d_desc d = *desc;
+  if (d.nx < 3 || d.ny < 3) return fail(JXF_ERR_INVALID, "grid must be at least 3x3");
+  if (!(d.dx > 0)) return fail(JXF_ERR_INVALID, "dx must be positive");
+  if (d.pml_layers < 0) return fail(JXF_ERR_INVALID, "pml_layers must be >= 0");
+  if (d.boundary != JXF_BND_ABSORBING && d.boundary != JXF_BND_PERIODIC &&
+      d.boundary != JXF_BND_REFLECTING && d.boundary != JXF_BND_PEC)
+    return fail(JXF_ERR_INVALID, "unsupported 2D boundary %d", d.boundary);
+  DeviceGuard dg(d.device);
+  if (!dg.ok) return fail(JXF_ERR_CUDA, "cannot select device %d", d.device);
+  jxf_grid2d* g = new jxf_grid2d();
+  g->d = d;
+  g->n = (long long)d.nx * d.ny;
+  g->dt = d.dt > 0 ? d.dt : 0.99 * d.dx / (kC0 * std::sqrt(2.0));  // fdtd.py:214
+  g->coef_h = g->dt / (kMu0 * d.dx);                                // fdtd.py:254
+  g->coef_e = g->dt / (kEps0 * d.dx);                               // fdtd.py:255
+  g->mode = d.boundary == JXF_BND_PERIODIC     ? MODE_PERIODIC
+            : d.boundary == JXF_BND_REFLECTING ? JXF_BND_REFLECTING
+                                               : MODE_ABSORB;
+  int rc;
+  for (int k = 0; k < 3; ++k) {
+    if ((rc = dmalloc(&g->f[k], (size_t)g->n, &g->bytes)) != JXF_OK) {
+      jxf_grid2d_destroy(g);
+      return rc;
+    }
+    cudaMemset(g->f[k], 0, (size_t)g->n * 4);
+  }
+  const int dims[2] = {d.nx, d.ny};
+  for (int ax = 0; ax < 2; ++ax) {
+    std::vector<float> t = d.boundary == JXF_BND_ABSORBING
+                               ? damping_table(dims[ax], d.pml_layers, d.dx, g->dt, 2)
+                               : std::vector<float>(dims[ax], 1.0f);
+    if ((rc = upload(&g->damp[ax], t, &g->bytes)) != JXF_OK) {
+      jxf_grid2d_destroy(g);
+      return rc;
+    }
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    jxf_grid2d_destroy(g);
+    return fail(JXF_ERR_CUDA, "initialisation failed: %s", cudaGetErrorString(e));
+  }
+  *out = g;
+  return JXF_OK;
+}
+
+int jxf_grid2d_destroy(jxf_grid2d* g) {
+  if (!g) return JXF_OK;
+  DeviceGuard dg(g->d.device);
+  for (int k = 0; k < 3; ++k) dfree(g->f[k]);
+  for (int k = 0; k < 2; ++k) dfree(g->damp[k]);
+  dfree(g->d_src_y);
+  dfree(g->d_src_amp);
+  dfree(g->d_src_wave);
+  dfree(g->d_wave);
+  dfree(g->d_wall_y);
+  dfree(g->d_wall_g0);
+  dfree(g->d_wall_g1);
+  delete g;
+  return JXF_OK;
+}
+
+int jxf_grid2d_set_sources(jxf_grid2d* g, int32_t n, const int32_t* y, const float* amplitude,
+                           const int32_t* wave_id) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n < 0 || (n > 0 && (!y || !amplitude || !wave_id)))
+    return fail(JXF_ERR_INVALID, "bad source arrays");
+  for (int i = 0; i < n; ++i) {
+    if (y[i] < 0 || y[i] >= g->d.ny)
+      return fail(JXF_ERR_INVALID, "source %d: y=%d out of grid bounds [0, %d)", i, y[i], g->d.ny);
+    if (wave_id[i] < 0) return fail(JXF_ERR_INVALID, "source %d: negative wave id", i);
+  }
+  DeviceGuard dg(g->d.device);
+  TRY(upload(&g->d_src_y, std::vector<int>(y, y + n), &g->bytes));
+  TRY(upload(&g->d_src_amp, std::vector<float>(amplitude, amplitude + n), &g->bytes));
+  TRY(upload(&g->d_src_wave, std::vector<int>(wave_id, wave_id + n), &g->bytes));
+  g->src_wave.assign(wave_id, wave_id + n);
+  g->n_src = n;
+  return JXF_OK;
+}
+
+int jxf_grid2d_set_waveforms(jxf_grid2d* g, int32_t n_waves, int64_t n_samples,
+                             const float* samples) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n_waves < 0 || n_samples < 0 || (n_waves * n_samples > 0 && !samples))
+    return fail(JXF_ERR_INVALID, "bad waveform table");
+  DeviceGuard dg(g->d.device);
+  TRY(upload(&g->d_wave, std::vector<float>(samples, samples + (size_t)n_waves * n_samples),
+             &g->bytes));
+  g->n_waves = n_waves;
+  g->wave_len = n_samples;
+  return JXF_OK;
+}
+
+int jxf_grid2d_set_walls(jxf_grid2d* g, int32_t n, const int32_t* y, const int32_t* gap_start,
+                         const int32_t* gap_end) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n < 0 || (n > 0 && (!y || !gap_start || !gap_end)))
+    return fail(JXF_ERR_INVALID, "bad wall arrays");
+  for (int i = 0; i < n; ++i)
+    if (y[i] < 0 || y[i] >= g->d.ny)
+      return fail(JXF_ERR_INVALID, "wall %d: y=%d out of grid bounds [0, %d)", i, y[i], g->d.ny);
+  DeviceGuard dg(g->d.device);
+  TRY(upload(&g->d_wall_y, std::vector<int>(y, y + n), &g->bytes));
+  TRY(upload(&g->d_wall_g0, std::vector<int>(gap_start, gap_start + n), &g->bytes));
+  TRY(upload(&g->d_wall_g1, std::vector<int>(gap_end, gap_end + n), &g->bytes));
+  g->n_wall = n;
+  return JXF_OK;
+}
+
+int jxf_grid2d_step(jxf_grid2d* g, int32_t n_steps, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n_steps < 0) return fail(JXF_ERR_INVALID, "n_steps must be >= 0");
+  if (n_steps == 0) return JXF_OK;
+  if (g->n_src > 0) {
+    int max_w = 0;
+    for (int w : g->src_wave) max_w = std::max(max_w, w);
+    if (max_w >= g->n_waves)
+      return fail(JXF_ERR_INVALID, "source wave id %d has no waveform row", max_w);
+    if (g->step + n_steps > g->wave_len)
+      return fail(JXF_ERR_INVALID, "waveform table covers %lld steps, need %lld", g->wave_len,
+                  g->step + n_steps);
+  }
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  Step2D p{};
+  p.nx = g->d.nx;
+  p.ny = g->d.ny;
+  p.a = (float)g->coef_h;
+  p.b = (float)g->coef_e;
+  p.ez = g->f[0];
+  p.hx = g->f[1];
+  p.hy = g->f[2];
+  p.damp[0] = g->damp[0];
+  p.damp[1] = g->damp[1];
+  p.n_src = g->n_src;
+  p.src_y = g->d_src_y;
+  p.src_amp = g->d_src_amp;
+  p.src_wave = g->d_src_wave;
+  p.wave = g->d_wave;
+  p.wave_len = g->wave_len;
+  p.n_wall = g->n_wall;
+  p.wall_y = g->d_wall_y;
+  p.wall_g0 = g->d_wall_g0;
+  p.wall_g1 = g->d_wall_g1;
+  const int threads = 256;
+  const int blocks = (int)std::min<long long>((g->n + threads - 1) / threads, 148LL * 16);
+  for (int k = 0; k < n_steps; ++k) {
+    p.step = g->step;
+    if (g->mode == MODE_PERIODIC) {
+      k2d_h<MODE_PERIODIC><<<blocks, threads, 0, st>>>(p);
+      k2d_e<MODE_PERIODIC, false><<<blocks, threads, 0, st>>>(p);
+      k2d_post<MODE_PERIODIC><<<1, 1024, 0, st>>>(p);
+    } else if (g->mode == JXF_BND_REFLECTING) {
+      k2d_h<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+      k2d_e<MODE_PEC, false><<<blocks, threads, 0, st>>>(p);
+      k2d_post<MODE_ABSORB><<<1, 1024, 0, st>>>(p);
+    } else {
+      k2d_h<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+      k2d_e<MODE_ABSORB, true><<<blocks, threads, 0, st>>>(p);
+    }
+    CUDA_TRY(cudaGetLastError());
+    g->step++;
+  }
+  return JXF_OK;
+}
+
+int jxf_grid2d_reset(jxf_grid2d* g, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(g->d.device);
+  for (int k = 0; k < 3; ++k)
+    CUDA_TRY(cudaMemsetAsync(g->f[k], 0, (size_t)g->n * 4, (cudaStream_t)stream));
+  g->step = 0;
+  return JXF_OK;
+}
+
+int jxf_grid2d_field_ptr(jxf_grid2d* g, int32_t comp, float** out) {
+  if (!g || !out) return fail(JXF_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 2) return fail(JXF_ERR_INVALID, "comp must be 0..2");
+  *out = g->f[comp];
+  return JXF_OK;
+}
+
+int jxf_grid2d_get_field(jxf_grid2d* g, int32_t comp, float* dst, int32_t dst_is_host,
+                         void* stream) {
+  if (!g || !dst) return fail(JXF_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 2) return fail(JXF_ERR_INVALID, "comp must be 0..2");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(dst, g->f[comp], (size_t)g->n * 4,
+                           dst_is_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
+  if (dst_is_host) CUDA_TRY(cudaStreamSynchronize(st));
+  return JXF_OK;
+}
+
+int jxf_grid2d_set_field(jxf_grid2d* g, int32_t comp, const float* src, int32_t src_is_host,
+                         void* stream) {
+  if (!g || !src) return fail(JXF_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 2) return fail(JXF_ERR_INVALID, "comp must be 0..2");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(g->f[comp], src, (size_t)g->n * 4,
+                           src_is_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+  if (src_is_host) CUDA_TRY(cudaStreamSynchronize(st));
+  return JXF_OK;
+}
+
+int jxf_grid2d_snapshot(jxf_grid2d* g, float* dst, void* stream) {
+  if (!g || !dst) return fail(JXF_ERR_INVALID, "null argument");
+  DeviceGuard dg(g->d.device);
+  for (int k = 0; k < 3; ++k)
+    CUDA_TRY(cudaMemcpyAsync(dst + (size_t)k * g->n, g->f[k], (size_t)g->n * 4,
+                             cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return JXF_OK;
+}
+
+int jxf_grid2d_check_error(jxf_grid2d* g, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(g->d.device);
+  CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+}  // extern "C"

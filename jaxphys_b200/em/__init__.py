@@ -1,0 +1,16 @@
+"""Electromagnetism: the FDTD Maxwell solvers (2D TM and 3D)."""
+
+from .fdtd import FDTD2D, EMGrid, PlaneWave, Wall
+from .fdtd3d import FDTD3D, CPMLSpec, DielectricRegion, EMGrid3D, PointSource3D
+
+__all__ = [
+    "EMGrid",
+    "PlaneWave",
+    "Wall",
+    "FDTD2D",
+    "EMGrid3D",
+    "PointSource3D",
+    "DielectricRegion",
+    "CPMLSpec",
+    "FDTD3D",
+]
