@@ -199,7 +199,7 @@ struct TmaConfig {
   int tz, ty, ry, stages;
   int threads;
   size_t smem[2];     // [mode: 0 absorb, 1 cpml]
-  TmaKernel k[2][2];  // [mode: 0 absorb, 1 cpml][cbarr]
+  TmaKernel k[3][2];  // [0 absorb, 1 cpml (kappa = 1), 2 cpml (kappa > 1)][cbarr]
 };
 
 template <int TZ, int TY, int RY, int ST>
@@ -212,10 +212,12 @@ TmaConfig make_cfg() {
   c.threads = TZ * (TY / RY);
   c.smem[0] = TmaLayout<TZ, TY, RY, ST, true, false>::SMEM_BYTES;
   c.smem[1] = TmaLayout<TZ, TY, RY, ST, true, true>::SMEM_BYTES;
-  c.k[0][0] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, false>;
-  c.k[0][1] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, true>;
-  c.k[1][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false>;
-  c.k[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true>;
+  c.k[0][0] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, false, false>;
+  c.k[0][1] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, true, false>;
+  c.k[1][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false>;
+  c.k[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false>;
+  c.k[2][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, true>;
+  c.k[2][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, true>;
   return c;
 }
 
@@ -240,6 +242,7 @@ std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
 struct jxf_grid3d {
   jxf_grid3d_desc d{};
   int mode = MODE_ABSORB;   // kernel mode: ABSORB (also PEC with unit tables), PERIODIC, CPML
+  bool kappa = false;       // CPML with kappa_max > 1 (1/kappa factors are not all 1)
   int path = JXF_PATH_GENERIC;
   double dt = 0, coef_h = 0, coef_e = 0;
   long long n = 0;
@@ -435,7 +438,8 @@ int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStr
                 g->maps_cfg, cfg);
   const TmaConfig& c = tma_configs()[cfg];
   const int mi = g->mode == MODE_CPML ? 1 : 0;
-  TmaKernel k = c.k[mi][g->cb ? 1 : 0];
+  const int ki = g->mode == MODE_CPML ? (g->kappa ? 2 : 1) : 0;
+  TmaKernel k = c.k[ki][g->cb ? 1 : 0];
   const size_t smem = c.smem[mi];
   static std::mutex mu;
   {
@@ -462,7 +466,8 @@ int heuristic_tune(jxf_grid3d* g) {
 // Time every (config, chunk) on A -> B launches (the state in A and the step
 // counter are untouched, probes off) and keep the fastest.
 int autotune(jxf_grid3d* g, cudaStream_t st) {
-  const auto key = std::make_tuple(g->d.nx, g->d.ny, g->d.nz, g->mode, g->cb ? 1 : 0);
+  const auto key =
+      std::make_tuple(g->d.nx, g->d.ny, g->d.nz, g->mode * 2 + (g->kappa ? 1 : 0), g->cb ? 1 : 0);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -600,6 +605,7 @@ int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out) {
   if (g->mode == MODE_CPML) {
     const double m = d.cpml_order > 0 ? d.cpml_order : 3.0;
     const double kmax = d.cpml_kappa_max >= 1.0 ? d.cpml_kappa_max : 1.0;
+    g->kappa = kmax > 1.0;
     for (int ax = 0; ax < 3; ++ax) {
       std::vector<float> t[TAB_COUNT];
       cpml_tables(dims[ax], d.pml_layers, d.dx, g->dt, m, d.cpml_r0, kmax, d.cpml_alpha_max, t);

@@ -38,11 +38,6 @@ __device__ __forceinline__ float h_plain(float h, float a, float d1, float d2) {
 __device__ __forceinline__ float e_plain(float e, float cb, float d1, float d2) {
   return fadd(e, fmul(cb, fsub(d1, d2)));
 }
-// CPML curl term: (ik1*d1 - ik2*d2) + (psi1 - psi2)
-__device__ __forceinline__ float cpml_curl(float ik1, float d1, float ik2, float d2, float p1,
-                                           float p2) {
-  return fadd(fsub(fmul(ik1, d1), fmul(ik2, d2)), fsub(p1, p2));
-}
 // psi <- b*psi + c*d
 __device__ __forceinline__ float psi_next(float b, float psi, float c, float d) {
   return fadd(fmul(b, psi), fmul(c, d));
@@ -58,23 +53,103 @@ __device__ __forceinline__ long long zs_index(int x, int y, int km, int ny, int 
   return ((long long)x * ny + y) * L2 + km;
 }
 
-// One CPML psi term for position `pos` on `axis` with slab index `m`
-// (m < 0: outside the slab, psi = 0).  Reads psi_in, writes psi_out if
-// `write`.
-__device__ __forceinline__ float psi_term(const CpmlDev& P, int id, int axis, int tb, int tc,
-                                          int pos, long long idx, bool in_slab, float d,
-                                          bool write) {
-  if (!in_slab) return 0.0f;
-  const float b = __ldg(P.tab[axis][tb] + pos);
-  const float c = __ldg(P.tab[axis][tc] + pos);
-  const float v = psi_next(b, P.in[id][idx], c, d);
-  if (write) P.out[id][idx] = v;
-  return v;
+template <bool B>
+struct BoolC {
+  static constexpr bool value = B;
+};
+
+// One CPML term of a field component: the derivative along one axis.
+struct PsiTerm {
+  bool on;     // cell inside this axis' slab (psi stored)
+  float b, c;  // recurrence coefficients at the component's position
+  float ik;    // 1/kappa at that position (1 outside the slab)
+  float old;   // psi_in (valid when on)
+  float* out;  // where to store the new psi, or nullptr
+};
+
+// curl' = (ik1 d1 - ik2 d2) + (psi1 - psi2), psi <- b psi + c d.
+// Outside both slabs the component uses the plain update instead (same value:
+// psi = 0 and ik = 1 there), so both kernels branch on the same condition.
+template <bool KAPPA>
+__device__ __forceinline__ float curl_cpml(float d1, float d2, const PsiTerm& t1,
+                                           const PsiTerm& t2) {
+  float p1 = 0.0f, p2 = 0.0f;
+  if (t1.on) {
+    p1 = psi_next(t1.b, t1.old, t1.c, d1);
+    if (t1.out) *t1.out = p1;
+  }
+  if (t2.on) {
+    p2 = psi_next(t2.b, t2.old, t2.c, d2);
+    if (t2.out) *t2.out = p2;
+  }
+  const float u1 = KAPPA ? fmul(t1.ik, d1) : d1;
+  const float u2 = KAPPA ? fmul(t2.ik, d2) : d2;
+  return fadd(fsub(u1, u2), fsub(p1, p2));
+}
+template <bool KAPPA>
+__device__ __forceinline__ float h_cpml(float h, float a, float d1, float d2, const PsiTerm& t1,
+                                        const PsiTerm& t2) {
+  if (!(t1.on || t2.on)) return h_plain(h, a, d1, d2);
+  return fsub(h, fmul(a, curl_cpml<KAPPA>(d1, d2, t1, t2)));
+}
+template <bool KAPPA>
+__device__ __forceinline__ float e_cpml(float e, float cb, float d1, float d2, const PsiTerm& t1,
+                                        const PsiTerm& t2) {
+  if (!(t1.on || t2.on)) return e_plain(e, cb, d1, d2);
+  return fadd(e, fmul(cb, curl_cpml<KAPPA>(d1, d2, t1, t2)));
+}
+
+// Coefficients of one position on one axis (H: half-integer, E: integer).
+struct AxisCoef {
+  float bh, ch, ikh, be, ce, ike;
+};
+__device__ __forceinline__ AxisCoef axis_coef(const CpmlDev& P, int axis, int pos) {
+  AxisCoef c;
+  c.bh = __ldg(P.tab[axis][TAB_BH] + pos);
+  c.ch = __ldg(P.tab[axis][TAB_CH] + pos);
+  c.ikh = __ldg(P.tab[axis][TAB_IKH] + pos);
+  c.be = __ldg(P.tab[axis][TAB_BE] + pos);
+  c.ce = __ldg(P.tab[axis][TAB_CE] + pos);
+  c.ike = __ldg(P.tab[axis][TAB_IKE] + pos);
+  return c;
+}
+// Term with coefficients loaded only when the cell is in the slab.
+__device__ __forceinline__ PsiTerm term_h_at(const CpmlDev& P, int axis, int pos, bool on,
+                                             float old, float* out) {
+  PsiTerm t{on, 0.0f, 0.0f, 1.0f, old, out};
+  if (on) {
+    t.b = __ldg(P.tab[axis][TAB_BH] + pos);
+    t.c = __ldg(P.tab[axis][TAB_CH] + pos);
+    t.ik = __ldg(P.tab[axis][TAB_IKH] + pos);
+  }
+  return t;
+}
+__device__ __forceinline__ PsiTerm term_e_at(const CpmlDev& P, int axis, int pos, bool on,
+                                             float old, float* out) {
+  PsiTerm t{on, 0.0f, 0.0f, 1.0f, old, out};
+  if (on) {
+    t.b = __ldg(P.tab[axis][TAB_BE] + pos);
+    t.c = __ldg(P.tab[axis][TAB_CE] + pos);
+    t.ik = __ldg(P.tab[axis][TAB_IKE] + pos);
+  }
+  return t;
+}
+__device__ __forceinline__ PsiTerm term_h(bool on, const AxisCoef& c, float old, float* out) {
+  return PsiTerm{on, c.bh, c.ch, c.ikh, old, out};
+}
+__device__ __forceinline__ PsiTerm term_e(bool on, const AxisCoef& c, float old, float* out) {
+  return PsiTerm{on, c.be, c.ce, c.ike, old, out};
 }
 
 // ---------------------------------------------------------------------------
 // generic path
 // ---------------------------------------------------------------------------
+
+// psi term read/written in place in global memory (generic kernels)
+__device__ __forceinline__ PsiTerm g_term(const CpmlDev& P, int id, bool on, float b, float c,
+                                          float ik, long long idx) {
+  return PsiTerm{on, b, c, ik, on ? P.out[id][idx] : 0.0f, on ? P.out[id] + idx : nullptr};
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Step3D p) {
@@ -106,53 +181,45 @@ __global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Ste
       uz = (x < nx - 1) && (y < ny - 1);
     }
     const float exc = ex[idx], eyc = ey[idx], ezc = ez[idx];
+    int im = -1, jm = -1, km = -1;
+    AxisCoef cx{}, cy{}, cz{};
+    if (MODE == MODE_CPML) {
+      im = slab_map(x, nx, p.pml.P[0]);
+      jm = slab_map(y, ny, p.pml.P[1]);
+      km = slab_map(z, nz, p.pml.P[2]);
+      cx = axis_coef(p.pml, 0, x);
+      cy = axis_coef(p.pml, 1, y);
+      cz = axis_coef(p.pml, 2, z);
+    }
+    const long long ix = xs_index(im, y, z, ny, nz);
+    const long long iy = ys_index(x, jm, z, p.pml.L[1], nz);
+    const long long iz = zs_index(x, y, km, ny, p.pml.L[2]);
     if (ux) {
       const float d1 = fsub(ez[iyp], ezc), d2 = fsub(ey[izp], eyc);
-      float h = p.in[3][idx];
-      if (MODE == MODE_CPML) {
-        const int jm = slab_map(y, ny, p.pml.P[1]), km = slab_map(z, nz, p.pml.P[2]);
-        const float p1 = psi_term(p.pml, PSI_HXY, 1, TAB_BH, TAB_CH, y,
-                                  ys_index(x, jm, z, p.pml.L[1], nz), jm >= 0, d1, true);
-        const float p2 = psi_term(p.pml, PSI_HXZ, 2, TAB_BH, TAB_CH, z,
-                                  zs_index(x, y, km, ny, p.pml.L[2]), km >= 0, d2, true);
-        h = fsub(h, fmul(a, cpml_curl(__ldg(p.pml.tab[1][TAB_IKH] + y), d1,
-                                      __ldg(p.pml.tab[2][TAB_IKH] + z), d2, p1, p2)));
-      } else {
-        h = h_plain(h, a, d1, d2);
-      }
-      p.out[3][idx] = h;
+      const float h = p.in[3][idx];
+      p.out[3][idx] =
+          MODE == MODE_CPML
+              ? h_cpml<true>(h, a, d1, d2, g_term(p.pml, PSI_HXY, jm >= 0, cy.bh, cy.ch, cy.ikh, iy),
+                             g_term(p.pml, PSI_HXZ, km >= 0, cz.bh, cz.ch, cz.ikh, iz))
+              : h_plain(h, a, d1, d2);
     }
     if (uy) {
       const float d1 = fsub(ex[izp], exc), d2 = fsub(ez[ixp], ezc);
-      float h = p.in[4][idx];
-      if (MODE == MODE_CPML) {
-        const int km = slab_map(z, nz, p.pml.P[2]), im = slab_map(x, nx, p.pml.P[0]);
-        const float p1 = psi_term(p.pml, PSI_HYZ, 2, TAB_BH, TAB_CH, z,
-                                  zs_index(x, y, km, ny, p.pml.L[2]), km >= 0, d1, true);
-        const float p2 = psi_term(p.pml, PSI_HYX, 0, TAB_BH, TAB_CH, x,
-                                  xs_index(im, y, z, ny, nz), im >= 0, d2, true);
-        h = fsub(h, fmul(a, cpml_curl(__ldg(p.pml.tab[2][TAB_IKH] + z), d1,
-                                      __ldg(p.pml.tab[0][TAB_IKH] + x), d2, p1, p2)));
-      } else {
-        h = h_plain(h, a, d1, d2);
-      }
-      p.out[4][idx] = h;
+      const float h = p.in[4][idx];
+      p.out[4][idx] =
+          MODE == MODE_CPML
+              ? h_cpml<true>(h, a, d1, d2, g_term(p.pml, PSI_HYZ, km >= 0, cz.bh, cz.ch, cz.ikh, iz),
+                             g_term(p.pml, PSI_HYX, im >= 0, cx.bh, cx.ch, cx.ikh, ix))
+              : h_plain(h, a, d1, d2);
     }
     if (uz) {
       const float d1 = fsub(ey[ixp], eyc), d2 = fsub(ex[iyp], exc);
-      float h = p.in[5][idx];
-      if (MODE == MODE_CPML) {
-        const int im = slab_map(x, nx, p.pml.P[0]), jm = slab_map(y, ny, p.pml.P[1]);
-        const float p1 = psi_term(p.pml, PSI_HZX, 0, TAB_BH, TAB_CH, x,
-                                  xs_index(im, y, z, ny, nz), im >= 0, d1, true);
-        const float p2 = psi_term(p.pml, PSI_HZY, 1, TAB_BH, TAB_CH, y,
-                                  ys_index(x, jm, z, p.pml.L[1], nz), jm >= 0, d2, true);
-        h = fsub(h, fmul(a, cpml_curl(__ldg(p.pml.tab[0][TAB_IKH] + x), d1,
-                                      __ldg(p.pml.tab[1][TAB_IKH] + y), d2, p1, p2)));
-      } else {
-        h = h_plain(h, a, d1, d2);
-      }
-      p.out[5][idx] = h;
+      const float h = p.in[5][idx];
+      p.out[5][idx] =
+          MODE == MODE_CPML
+              ? h_cpml<true>(h, a, d1, d2, g_term(p.pml, PSI_HZX, im >= 0, cx.bh, cx.ch, cx.ikh, ix),
+                             g_term(p.pml, PSI_HZY, jm >= 0, cy.bh, cy.ch, cy.ikh, iy))
+              : h_plain(h, a, d1, d2);
     }
   }
 }
@@ -188,47 +255,39 @@ __global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Ste
     const float cb = p.cb ? p.cb[idx] : p.cb_const;
     const float hxc = hx[idx], hyc = hy[idx], hzc = hz[idx];
     float ex = p.in[0][idx], ey = p.in[1][idx], ez = p.in[2][idx];
+    int im = -1, jm = -1, km = -1;
+    AxisCoef cx{}, cy{}, cz{};
+    if (MODE == MODE_CPML) {
+      im = slab_map(x, nx, p.pml.P[0]);
+      jm = slab_map(y, ny, p.pml.P[1]);
+      km = slab_map(z, nz, p.pml.P[2]);
+      cx = axis_coef(p.pml, 0, x);
+      cy = axis_coef(p.pml, 1, y);
+      cz = axis_coef(p.pml, 2, z);
+    }
+    const long long ix = xs_index(im, y, z, ny, nz);
+    const long long iy = ys_index(x, jm, z, p.pml.L[1], nz);
+    const long long iz = zs_index(x, y, km, ny, p.pml.L[2]);
     if (ux) {
       const float d1 = fsub(hzc, hz[iym]), d2 = fsub(hyc, hy[izm]);
-      if (MODE == MODE_CPML) {
-        const int jm = slab_map(y, ny, p.pml.P[1]), km = slab_map(z, nz, p.pml.P[2]);
-        const float p1 = psi_term(p.pml, PSI_EXY, 1, TAB_BE, TAB_CE, y,
-                                  ys_index(x, jm, z, p.pml.L[1], nz), jm >= 0, d1, true);
-        const float p2 = psi_term(p.pml, PSI_EXZ, 2, TAB_BE, TAB_CE, z,
-                                  zs_index(x, y, km, ny, p.pml.L[2]), km >= 0, d2, true);
-        ex = fadd(ex, fmul(cb, cpml_curl(__ldg(p.pml.tab[1][TAB_IKE] + y), d1,
-                                         __ldg(p.pml.tab[2][TAB_IKE] + z), d2, p1, p2)));
-      } else {
-        ex = e_plain(ex, cb, d1, d2);
-      }
+      ex = MODE == MODE_CPML
+               ? e_cpml<true>(ex, cb, d1, d2, g_term(p.pml, PSI_EXY, jm >= 0, cy.be, cy.ce, cy.ike, iy),
+                              g_term(p.pml, PSI_EXZ, km >= 0, cz.be, cz.ce, cz.ike, iz))
+               : e_plain(ex, cb, d1, d2);
     }
     if (uy) {
       const float d1 = fsub(hxc, hx[izm]), d2 = fsub(hzc, hz[ixm]);
-      if (MODE == MODE_CPML) {
-        const int km = slab_map(z, nz, p.pml.P[2]), im = slab_map(x, nx, p.pml.P[0]);
-        const float p1 = psi_term(p.pml, PSI_EYZ, 2, TAB_BE, TAB_CE, z,
-                                  zs_index(x, y, km, ny, p.pml.L[2]), km >= 0, d1, true);
-        const float p2 = psi_term(p.pml, PSI_EYX, 0, TAB_BE, TAB_CE, x,
-                                  xs_index(im, y, z, ny, nz), im >= 0, d2, true);
-        ey = fadd(ey, fmul(cb, cpml_curl(__ldg(p.pml.tab[2][TAB_IKE] + z), d1,
-                                         __ldg(p.pml.tab[0][TAB_IKE] + x), d2, p1, p2)));
-      } else {
-        ey = e_plain(ey, cb, d1, d2);
-      }
+      ey = MODE == MODE_CPML
+               ? e_cpml<true>(ey, cb, d1, d2, g_term(p.pml, PSI_EYZ, km >= 0, cz.be, cz.ce, cz.ike, iz),
+                              g_term(p.pml, PSI_EYX, im >= 0, cx.be, cx.ce, cx.ike, ix))
+               : e_plain(ey, cb, d1, d2);
     }
     if (uz) {
       const float d1 = fsub(hyc, hy[ixm]), d2 = fsub(hxc, hx[iym]);
-      if (MODE == MODE_CPML) {
-        const int im = slab_map(x, nx, p.pml.P[0]), jm = slab_map(y, ny, p.pml.P[1]);
-        const float p1 = psi_term(p.pml, PSI_EZX, 0, TAB_BE, TAB_CE, x,
-                                  xs_index(im, y, z, ny, nz), im >= 0, d1, true);
-        const float p2 = psi_term(p.pml, PSI_EZY, 1, TAB_BE, TAB_CE, y,
-                                  ys_index(x, jm, z, p.pml.L[1], nz), jm >= 0, d2, true);
-        ez = fadd(ez, fmul(cb, cpml_curl(__ldg(p.pml.tab[0][TAB_IKE] + x), d1,
-                                         __ldg(p.pml.tab[1][TAB_IKE] + y), d2, p1, p2)));
-      } else {
-        ez = e_plain(ez, cb, d1, d2);
-      }
+      ez = MODE == MODE_CPML
+               ? e_cpml<true>(ez, cb, d1, d2, g_term(p.pml, PSI_EZX, im >= 0, cx.be, cx.ce, cx.ike, ix),
+                              g_term(p.pml, PSI_EZY, jm >= 0, cy.be, cy.ce, cy.ike, iy))
+               : e_plain(ez, cb, d1, d2);
     }
     if (MODE == MODE_ABSORB) {
       const float f = fmul(fmul(__ldg(p.damp[0] + x), __ldg(p.damp[1] + y)), __ldg(p.damp[2] + z));
@@ -298,7 +357,7 @@ struct TmaLayout {
   // CPML: psi of the current and next plane, per thread: 12 core values per
   // row and 4 halo values (double buffered).
   static constexpr int PSC_FLOATS = CPML ? 2 * PSI_COUNT * RY * NT : 0;
-  static constexpr int PSH_FLOATS = CPML ? 2 * 4 * NT : 0;
+  static constexpr int PSH_FLOATS = CPML ? 2 * 4 * (TZ + TY) : 0;
   static constexpr size_t SMEM_BYTES =
       128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + 3 * (size_t)HN_STRIDE +
                              PSC_FLOATS + PSH_FLOATS);
@@ -310,26 +369,14 @@ struct TmaLayout {
   static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per block exceeds 227 KB");
 };
 
-// psi update from a prefetched old value: b*old + c*d, written to psi_out
-// when `write`; 0 outside the slab.
-__device__ __forceinline__ float psi_from(const CpmlDev& P, int id, int axis, int tb, int tc,
-                                          int pos, long long idx, bool in_slab, float d,
-                                          bool write, float old) {
-  if (!in_slab) return 0.0f;
-  const float b = __ldg(P.tab[axis][tb] + pos);
-  const float c = __ldg(P.tab[axis][tc] + pos);
-  const float v = psi_next(b, old, c, d);
-  if (write) P.out[id][idx] = v;
-  return v;
-}
-
-template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR>
+template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA>
 __global__ void __launch_bounds__(TZ*(TY / RY))
     k3d_tma(const __grid_constant__ Step3D p, const __grid_constant__ Maps3D maps) {
   constexpr bool CPML = (MODE == MODE_CPML);
   using L = TmaLayout<TZ, TY, RY, STAGES, CBARR, CPML>;
   constexpr int TYT = L::TYT;
   constexpr int NT = L::NT;
+  constexpr int NH = TZ + TY;  // halo threads
   constexpr int EW = L::EW, HW = L::HW, NW = L::NW;
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -389,13 +436,16 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   }
   int issued = min(STAGES, nload);  // identical in every thread
 
-  // ---- CPML: slab coordinates of this thread's cells (fixed over the march)
+  // ---- CPML: slab coordinates and coefficients of this thread's cells
+  // (fixed over the march along x)
   int jm_r[RY];
   int km = -1;
-  int jm_h = -1, km_h = -1;   // halo cell
-  int yh = -1, zh = -1;       // halo cell coordinates (-1: none)
+  AxisCoef cz{};
+  int jm_h = -1, km_h = -1;  // halo cell slab indices
+  int yh = -1, zh = -1;      // halo cell (-1: none)
   if (CPML) {
     km = (z < nz) ? slab_map(z, nz, p.pml.P[2]) : -1;
+    if (z < nz) cz = axis_coef(p.pml, 2, z);
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       const int y = y0 + ty + r * TYT;
@@ -406,7 +456,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
         yh = y0 - 1;
         zh = z0 + tid;
       }
-    } else if (tid < TZ + TY) {  // column halo (y0+tid-TZ, z0-1)
+    } else if (tid < NH) {  // column halo (y0+tid-TZ, z0-1)
       if (z0 >= 1 && y0 + tid - TZ < ny) {
         yh = y0 + tid - TZ;
         zh = z0 - 1;
@@ -418,7 +468,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     }
   }
 #define PSC(buf, id, r) PSc[(((buf) * PSI_COUNT + (id)) * RY + (r)) * NT + tid]
-#define PSH(buf, k) PSh[((buf) * 4 + (k)) * NT + tid]
+#define PSH(buf, k) PSh[((buf) * 4 + (k)) * NH + tid]
   // Prefetch psi_in of plane q into buffer `buf` (this thread's cells only).
   auto issue_psi = [&](int q, int buf) {
     const int imq = slab_map(q, nx, p.pml.P[0]);
@@ -513,7 +563,13 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
 #define H_AT(c, yy, zc) Hs[(c) * L::H_STRIDE + (yy) * HW + (zc)]
 #define HN_AT(c, yy, zc) Hn[(c) * L::HN_STRIDE + (yy) * NW + (zc)]
     const bool warm = (x < xb);
-    const int imx = CPML ? slab_map(x, nx, p.pml.P[0]) : -1;
+    int imx = -1;
+    AxisCoef cx{};
+    if (CPML) {
+      imx = slab_map(x, nx, p.pml.P[0]);
+      cx = axis_coef(p.pml, 0, x);
+    }
+    const bool inx = imx >= 0;
 
     // ---------------- H^{n+1/2} on the tile (registers + Hn) ----------------
     float exr[RY], eyr[RY], ezr[RY], hxr[RY], hyr[RY], hzr[RY];
@@ -528,53 +584,49 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       eyr[r] = eyc;
       ezr[r] = ezc;
       float hx = H_AT(0, yy, zz), hy = H_AT(1, yy, zz), hz = H_AT(2, yy, zz);
-      if (!warm && y < ny - 1 && z < nz - 1) {  // Hx
-        const float d1 = fsub(E_AT(2, yy + 1, zz), ezc), d2 = fsub(E_AT(1, yy, zz + 1), eyc);
-        if (CPML) {
-          const int jm = jm_r[r];
-          const float p1 = psi_from(p.pml, PSI_HXY, 1, TAB_BH, TAB_CH, y,
-                                    ys_index(x, jm, z, p.pml.L[1], nz), jm >= 0, d1, own,
-                                    PSC(pb, PSI_HXY, r));
-          const float p2 = psi_from(p.pml, PSI_HXZ, 2, TAB_BH, TAB_CH, z,
-                                    zs_index(x, y, km, ny, p.pml.L[2]), km >= 0, d2, own,
-                                    PSC(pb, PSI_HXZ, r));
-          hx = fsub(hx, fmul(a, cpml_curl(__ldg(p.pml.tab[1][TAB_IKH] + y), d1,
-                                          __ldg(p.pml.tab[2][TAB_IKH] + z), d2, p1, p2)));
-        } else {
-          hx = h_plain(hx, a, d1, d2);
+      const bool iny = CPML && jm_r[r] >= 0, inz = CPML && km >= 0;
+      // Cells outside every slab take the plain update (identical value: psi
+      // is 0 and 1/kappa is 1 there) without touching any CPML state.
+      auto h_phase = [&](auto cpm) {
+        constexpr bool CP = decltype(cpm)::value;
+        const long long ix = CP ? xs_index(imx, y, z, ny, nz) : 0;
+        const long long iy = CP ? ys_index(x, jm_r[r], z, p.pml.L[1], nz) : 0;
+        const long long iz = CP ? zs_index(x, y, km, ny, p.pml.L[2]) : 0;
+        if (!warm && y < ny - 1 && z < nz - 1) {  // Hx: d/dy Ez - d/dz Ey
+          const float d1 = fsub(E_AT(2, yy + 1, zz), ezc), d2 = fsub(E_AT(1, yy, zz + 1), eyc);
+          if (CP)
+            hx = h_cpml<KAPPA>(
+                hx, a, d1, d2,
+                term_h_at(p.pml, 1, y, iny, PSC(pb, PSI_HXY, r), own ? p.pml.out[PSI_HXY] + iy : nullptr),
+                term_h(inz, cz, PSC(pb, PSI_HXZ, r), own ? p.pml.out[PSI_HXZ] + iz : nullptr));
+          else
+            hx = h_plain(hx, a, d1, d2);
         }
-      }
-      if (x < nx - 1 && z < nz - 1 && y < ny) {  // Hy
-        const float d1 = fsub(E_AT(0, yy, zz + 1), exc), d2 = fsub(EN_AT(2, yy, zz), ezc);
-        if (CPML) {
-          const float p1 = psi_from(p.pml, PSI_HYZ, 2, TAB_BH, TAB_CH, z,
-                                    zs_index(x, y, km, ny, p.pml.L[2]), km >= 0, d1, own,
-                                    PSC(pb, PSI_HYZ, r));
-          const float p2 = psi_from(p.pml, PSI_HYX, 0, TAB_BH, TAB_CH, x,
-                                    xs_index(imx, y, z, ny, nz), imx >= 0, d2, own,
-                                    PSC(pb, PSI_HYX, r));
-          hy = fsub(hy, fmul(a, cpml_curl(__ldg(p.pml.tab[2][TAB_IKH] + z), d1,
-                                          __ldg(p.pml.tab[0][TAB_IKH] + x), d2, p1, p2)));
-        } else {
-          hy = h_plain(hy, a, d1, d2);
+        if (x < nx - 1 && z < nz - 1 && y < ny) {  // Hy: d/dz Ex - d/dx Ez
+          const float d1 = fsub(E_AT(0, yy, zz + 1), exc), d2 = fsub(EN_AT(2, yy, zz), ezc);
+          if (CP)
+            hy = h_cpml<KAPPA>(
+                hy, a, d1, d2,
+                term_h(inz, cz, PSC(pb, PSI_HYZ, r), own ? p.pml.out[PSI_HYZ] + iz : nullptr),
+                term_h(inx, cx, PSC(pb, PSI_HYX, r), own ? p.pml.out[PSI_HYX] + ix : nullptr));
+          else
+            hy = h_plain(hy, a, d1, d2);
         }
-      }
-      if (x < nx - 1 && y < ny - 1 && z < nz) {  // Hz
-        const float d1 = fsub(EN_AT(1, yy, zz), eyc), d2 = fsub(E_AT(0, yy + 1, zz), exc);
-        if (CPML) {
-          const int jm = jm_r[r];
-          const float p1 = psi_from(p.pml, PSI_HZX, 0, TAB_BH, TAB_CH, x,
-                                    xs_index(imx, y, z, ny, nz), imx >= 0, d1, own,
-                                    PSC(pb, PSI_HZX, r));
-          const float p2 = psi_from(p.pml, PSI_HZY, 1, TAB_BH, TAB_CH, y,
-                                    ys_index(x, jm, z, p.pml.L[1], nz), jm >= 0, d2, own,
-                                    PSC(pb, PSI_HZY, r));
-          hz = fsub(hz, fmul(a, cpml_curl(__ldg(p.pml.tab[0][TAB_IKH] + x), d1,
-                                          __ldg(p.pml.tab[1][TAB_IKH] + y), d2, p1, p2)));
-        } else {
-          hz = h_plain(hz, a, d1, d2);
+        if (x < nx - 1 && y < ny - 1 && z < nz) {  // Hz: d/dx Ey - d/dy Ex
+          const float d1 = fsub(EN_AT(1, yy, zz), eyc), d2 = fsub(E_AT(0, yy + 1, zz), exc);
+          if (CP)
+            hz = h_cpml<KAPPA>(
+                hz, a, d1, d2,
+                term_h(inx, cx, PSC(pb, PSI_HZX, r), own ? p.pml.out[PSI_HZX] + ix : nullptr),
+                term_h_at(p.pml, 1, y, iny, PSC(pb, PSI_HZY, r), own ? p.pml.out[PSI_HZY] + iy : nullptr));
+          else
+            hz = h_plain(hz, a, d1, d2);
         }
-      }
+      };
+      if (CPML && (iny || inz || inx))
+        h_phase(BoolC<CPML>{});
+      else
+        h_phase(BoolC<false>{});
       hxr[r] = hx;
       hyr[r] = hy;
       hzr[r] = hz;
@@ -586,7 +638,8 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     }
 
     // ---------------- halo H: row y0-1 (Hx, Hz) and column z0-1 (Hx, Hy) ------
-    if (!warm && tid < TZ + TY) {
+    // recomputed from the staged E (the owner block writes these cells)
+    if (!warm && tid < NH) {
       if (tid < TZ) {
         const int y = y0 - 1;
         const int zc = z0 + tid;
@@ -596,29 +649,19 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
           const float ezc = E_AT(2, 0, zb), eyc = E_AT(1, 0, zb), exc = E_AT(0, 0, zb);
           if (zc < nz - 1) {  // y < ny-1 holds: y0 < ny
             const float d1 = fsub(E_AT(2, 1, zb), ezc), d2 = fsub(E_AT(1, 0, zb + 1), eyc);
-            if (CPML) {
-              const float p1 = psi_from(p.pml, PSI_HXY, 1, TAB_BH, TAB_CH, y, 0, jm_h >= 0, d1,
-                                        false, PSH(pb, 0));
-              const float p2 = psi_from(p.pml, PSI_HXZ, 2, TAB_BH, TAB_CH, zc, 0, km_h >= 0, d2,
-                                        false, PSH(pb, 1));
-              hx = fsub(hx, fmul(a, cpml_curl(__ldg(p.pml.tab[1][TAB_IKH] + y), d1,
-                                              __ldg(p.pml.tab[2][TAB_IKH] + zc), d2, p1, p2)));
-            } else {
+            if (CPML)
+              hx = h_cpml<KAPPA>(hx, a, d1, d2, term_h_at(p.pml, 1, y, jm_h >= 0, PSH(pb, 0), nullptr),
+                                 term_h_at(p.pml, 2, zc, km_h >= 0, PSH(pb, 1), nullptr));
+            else
               hx = h_plain(hx, a, d1, d2);
-            }
           }
           if (x < nx - 1) {
             const float d1 = fsub(EN_AT(1, 0, zb), eyc), d2 = fsub(E_AT(0, 1, zb), exc);
-            if (CPML) {
-              const float p1 = psi_from(p.pml, PSI_HZX, 0, TAB_BH, TAB_CH, x, 0, imx >= 0, d1,
-                                        false, PSH(pb, 2));
-              const float p2 = psi_from(p.pml, PSI_HZY, 1, TAB_BH, TAB_CH, y, 0, jm_h >= 0, d2,
-                                        false, PSH(pb, 3));
-              hz = fsub(hz, fmul(a, cpml_curl(__ldg(p.pml.tab[0][TAB_IKH] + x), d1,
-                                              __ldg(p.pml.tab[1][TAB_IKH] + y), d2, p1, p2)));
-            } else {
+            if (CPML)
+              hz = h_cpml<KAPPA>(hz, a, d1, d2, term_h(inx, cx, PSH(pb, 2), nullptr),
+                                 term_h_at(p.pml, 1, y, jm_h >= 0, PSH(pb, 3), nullptr));
+            else
               hz = h_plain(hz, a, d1, d2);
-            }
           }
         }
         HN_AT(0, 0, tid + 1) = hx;
@@ -633,29 +676,19 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
           const float ezc = E_AT(2, yy, 3), eyc = E_AT(1, yy, 3), exc = E_AT(0, yy, 3);
           if (y < ny - 1) {  // zc < nz-1 holds: z0 < nz
             const float d1 = fsub(E_AT(2, yy + 1, 3), ezc), d2 = fsub(E_AT(1, yy, 4), eyc);
-            if (CPML) {
-              const float p1 = psi_from(p.pml, PSI_HXY, 1, TAB_BH, TAB_CH, y, 0, jm_h >= 0, d1,
-                                        false, PSH(pb, 0));
-              const float p2 = psi_from(p.pml, PSI_HXZ, 2, TAB_BH, TAB_CH, zc, 0, km_h >= 0, d2,
-                                        false, PSH(pb, 1));
-              hx = fsub(hx, fmul(a, cpml_curl(__ldg(p.pml.tab[1][TAB_IKH] + y), d1,
-                                              __ldg(p.pml.tab[2][TAB_IKH] + zc), d2, p1, p2)));
-            } else {
+            if (CPML)
+              hx = h_cpml<KAPPA>(hx, a, d1, d2, term_h_at(p.pml, 1, y, jm_h >= 0, PSH(pb, 0), nullptr),
+                                 term_h_at(p.pml, 2, zc, km_h >= 0, PSH(pb, 1), nullptr));
+            else
               hx = h_plain(hx, a, d1, d2);
-            }
           }
           if (x < nx - 1) {
             const float d1 = fsub(E_AT(0, yy, 4), exc), d2 = fsub(EN_AT(2, yy, 3), ezc);
-            if (CPML) {
-              const float p1 = psi_from(p.pml, PSI_HYZ, 2, TAB_BH, TAB_CH, zc, 0, km_h >= 0, d1,
-                                        false, PSH(pb, 2));
-              const float p2 = psi_from(p.pml, PSI_HYX, 0, TAB_BH, TAB_CH, x, 0, imx >= 0, d2,
-                                        false, PSH(pb, 3));
-              hy = fsub(hy, fmul(a, cpml_curl(__ldg(p.pml.tab[2][TAB_IKH] + zc), d1,
-                                              __ldg(p.pml.tab[0][TAB_IKH] + x), d2, p1, p2)));
-            } else {
+            if (CPML)
+              hy = h_cpml<KAPPA>(hy, a, d1, d2, term_h_at(p.pml, 2, zc, km_h >= 0, PSH(pb, 2), nullptr),
+                                 term_h(inx, cx, PSH(pb, 3), nullptr));
+            else
               hy = h_plain(hy, a, d1, d2);
-            }
           }
         }
         HN_AT(0, yy, 0) = hx;
@@ -680,56 +713,45 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
         float ex = exr[r], ey = eyr[r], ez = ezr[r];
         const float hxc = hxr[r], hyc = hyr[r], hzc = hzr[r];
         const float cb = CBARR ? CBs[yl * TZ + tx] : p.cb_const;
-        if (y >= 1 && z >= 1) {  // Ex
-          const float d1 = fsub(hzc, HN_AT(2, yy - 1, zn)), d2 = fsub(hyc, HN_AT(1, yy, zn - 1));
-          if (CPML) {
-            const int jm = jm_r[r];
-            const float p1 = psi_from(p.pml, PSI_EXY, 1, TAB_BE, TAB_CE, y,
-                                      ys_index(x, jm, z, p.pml.L[1], nz), own && jm >= 0, d1, own,
-                                      PSC(pb, PSI_EXY, r));
-            const float p2 = psi_from(p.pml, PSI_EXZ, 2, TAB_BE, TAB_CE, z,
-                                      zs_index(x, y, km, ny, p.pml.L[2]), own && km >= 0, d2, own,
-                                      PSC(pb, PSI_EXZ, r));
-            if (own)
-              ex = fadd(ex, fmul(cb, cpml_curl(__ldg(p.pml.tab[1][TAB_IKE] + y), d1,
-                                               __ldg(p.pml.tab[2][TAB_IKE] + z), d2, p1, p2)));
-          } else {
-            ex = e_plain(ex, cb, d1, d2);
+        const bool iny = CPML && own && jm_r[r] >= 0, inz = CPML && own && km >= 0;
+        const bool inxo = own && inx;
+        auto e_phase = [&](auto cpm) {
+          constexpr bool CP = decltype(cpm)::value;
+          const long long ix = CP ? xs_index(imx, y, z, ny, nz) : 0;
+          const long long iy = CP ? ys_index(x, jm_r[r], z, p.pml.L[1], nz) : 0;
+          const long long iz = CP ? zs_index(x, y, km, ny, p.pml.L[2]) : 0;
+          if (y >= 1 && z >= 1) {  // Ex: d/dy Hz - d/dz Hy
+            const float d1 = fsub(hzc, HN_AT(2, yy - 1, zn)), d2 = fsub(hyc, HN_AT(1, yy, zn - 1));
+            if (CP)
+              ex = e_cpml<KAPPA>(ex, cb, d1, d2,
+                                 term_e_at(p.pml, 1, y, iny, PSC(pb, PSI_EXY, r), p.pml.out[PSI_EXY] + iy),
+                                 term_e(inz, cz, PSC(pb, PSI_EXZ, r), p.pml.out[PSI_EXZ] + iz));
+            else
+              ex = e_plain(ex, cb, d1, d2);
           }
-        }
-        if (x >= 1 && z >= 1) {  // Ey
-          const float d1 = fsub(hxc, HN_AT(0, yy, zn - 1)), d2 = fsub(hzc, hz_prev[r]);
-          if (CPML) {
-            const float p1 = psi_from(p.pml, PSI_EYZ, 2, TAB_BE, TAB_CE, z,
-                                      zs_index(x, y, km, ny, p.pml.L[2]), own && km >= 0, d1, own,
-                                      PSC(pb, PSI_EYZ, r));
-            const float p2 = psi_from(p.pml, PSI_EYX, 0, TAB_BE, TAB_CE, x,
-                                      xs_index(imx, y, z, ny, nz), own && imx >= 0, d2, own,
-                                      PSC(pb, PSI_EYX, r));
-            if (own)
-              ey = fadd(ey, fmul(cb, cpml_curl(__ldg(p.pml.tab[2][TAB_IKE] + z), d1,
-                                               __ldg(p.pml.tab[0][TAB_IKE] + x), d2, p1, p2)));
-          } else {
-            ey = e_plain(ey, cb, d1, d2);
+          if (x >= 1 && z >= 1) {  // Ey: d/dz Hx - d/dx Hz
+            const float d1 = fsub(hxc, HN_AT(0, yy, zn - 1)), d2 = fsub(hzc, hz_prev[r]);
+            if (CP)
+              ey = e_cpml<KAPPA>(ey, cb, d1, d2,
+                                 term_e(inz, cz, PSC(pb, PSI_EYZ, r), p.pml.out[PSI_EYZ] + iz),
+                                 term_e(inxo, cx, PSC(pb, PSI_EYX, r), p.pml.out[PSI_EYX] + ix));
+            else
+              ey = e_plain(ey, cb, d1, d2);
           }
-        }
-        if (x >= 1 && y >= 1) {  // Ez
-          const float d1 = fsub(hyc, hy_prev[r]), d2 = fsub(hxc, HN_AT(0, yy - 1, zn));
-          if (CPML) {
-            const int jm = jm_r[r];
-            const float p1 = psi_from(p.pml, PSI_EZX, 0, TAB_BE, TAB_CE, x,
-                                      xs_index(imx, y, z, ny, nz), own && imx >= 0, d1, own,
-                                      PSC(pb, PSI_EZX, r));
-            const float p2 = psi_from(p.pml, PSI_EZY, 1, TAB_BE, TAB_CE, y,
-                                      ys_index(x, jm, z, p.pml.L[1], nz), own && jm >= 0, d2, own,
-                                      PSC(pb, PSI_EZY, r));
-            if (own)
-              ez = fadd(ez, fmul(cb, cpml_curl(__ldg(p.pml.tab[0][TAB_IKE] + x), d1,
-                                               __ldg(p.pml.tab[1][TAB_IKE] + y), d2, p1, p2)));
-          } else {
-            ez = e_plain(ez, cb, d1, d2);
+          if (x >= 1 && y >= 1) {  // Ez: d/dx Hy - d/dy Hx
+            const float d1 = fsub(hyc, hy_prev[r]), d2 = fsub(hxc, HN_AT(0, yy - 1, zn));
+            if (CP)
+              ez = e_cpml<KAPPA>(ez, cb, d1, d2,
+                                 term_e(inxo, cx, PSC(pb, PSI_EZX, r), p.pml.out[PSI_EZX] + ix),
+                                 term_e_at(p.pml, 1, y, iny, PSC(pb, PSI_EZY, r), p.pml.out[PSI_EZY] + iy));
+            else
+              ez = e_plain(ez, cb, d1, d2);
           }
-        }
+        };
+        if (CPML && (iny || inz || inxo))
+          e_phase(BoolC<CPML>{});
+        else
+          e_phase(BoolC<false>{});
         if (MODE == MODE_ABSORB && own) {
           const float f =
               fmul(fmul(__ldg(p.damp[0] + x), __ldg(p.damp[1] + y)), __ldg(p.damp[2] + z));
