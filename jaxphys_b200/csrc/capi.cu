@@ -275,6 +275,13 @@ struct jxf_grid3d {
   int n_probes = 0;
   int* d_err = nullptr;
   int* d_count = nullptr;
+  // CPML region split: blocks that touch a psi slab (shell) run the CPML
+  // kernel, the others the plain kernel (compact block lists per launch shape)
+  int* d_shell = nullptr;
+  int* d_inner = nullptr;
+  int n_shell = 0, n_inner = 0;
+  int split_cfg = -1, split_chunk = -1;
+  bool use_pdl = true;  // programmatic dependent launch between step kernels
   // TMA selection
   int cfg = -1, x_chunk = 0;
   bool maps_ok = false;
@@ -430,15 +437,17 @@ void set_io(jxf_grid3d* g, Step3D& p, int in_set, int out_set) {
   }
 }
 
-int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStream_t st) {
+int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStream_t st,
+               int list_count, bool plain = false) {
   // The boxes of the tensor maps must be the ones this config's kernel expects
   // (the mbarrier transaction count is derived from them).
   if (!g->maps_ok || g->maps_cfg != cfg)
     return fail(JXF_ERR_INVALID, "tensor maps encoded for config %d, launching config %d",
                 g->maps_cfg, cfg);
   const TmaConfig& c = tma_configs()[cfg];
-  const int mi = g->mode == MODE_CPML ? 1 : 0;
-  const int ki = g->mode == MODE_CPML ? (g->kappa ? 2 : 1) : 0;
+  const bool cpml = g->mode == MODE_CPML && !plain;
+  const int mi = cpml ? 1 : 0;
+  const int ki = cpml ? (g->kappa ? 2 : 1) : 0;
   TmaKernel k = c.k[ki][g->cb ? 1 : 0];
   const size_t smem = c.smem[mi];
   static std::mutex mu;
@@ -450,8 +459,93 @@ int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStr
   p.ntiles_z = (g->d.nz + c.tz - 1) / c.tz;
   p.ntiles_y = (g->d.ny + c.ty - 1) / c.ty;
   dim3 grid(p.ntiles_z, p.ntiles_y, (g->d.nx + chunk - 1) / chunk);
-  k<<<grid, c.threads, smem, st>>>(p, g->maps[in_set]);
-  CUDA_TRY(cudaGetLastError());
+  if (list_count >= 0) grid = dim3(list_count, 1, 1);
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = grid;
+  lc.blockDim = dim3(c.threads, 1, 1);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = g->use_pdl ? 1 : 0;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&lc, k, p, g->maps[in_set]);
+  if (e != cudaSuccess && g->use_pdl) {
+    // stream without programmatic serialization support: launch in order
+    (void)cudaGetLastError();
+    g->use_pdl = false;
+    p.pdl = 0;
+    lc.numAttrs = 0;
+    e = cudaLaunchKernelEx(&lc, k, p, g->maps[in_set]);
+  }
+  if (e != cudaSuccess)
+    return fail(JXF_ERR_CUDA, "step kernel launch failed: %s", cudaGetErrorString(e));
+  return JXF_OK;
+}
+
+// A coordinate range [lo, hi] along an axis of length n avoids the slab
+// storage of half width P (P < 0: the whole axis is stored).
+bool range_clear(int lo, int hi, int n, int P) {
+  if (P < 0) return false;
+  lo = std::max(lo, 0);
+  hi = std::min(hi, n - 1);
+  return lo >= P && hi < n - P;
+}
+
+int build_split(jxf_grid3d* g, int cfg, int chunk) {
+  if (g->split_cfg == cfg && g->split_chunk == chunk) return JXF_OK;
+  const TmaConfig& c = tma_configs()[cfg];
+  const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
+  const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
+  const int nch = (nx + chunk - 1) / chunk;
+  std::vector<int> shell, inner;
+  for (int ch = 0; ch < nch; ++ch)
+    for (int ty = 0; ty < nty; ++ty)
+      for (int tz = 0; tz < ntz; ++tz) {
+        const int z0 = tz * c.tz, y0 = ty * c.ty, xb = ch * chunk;
+        const int xe = std::min(xb + chunk, nx);
+        // cells of the tile, its halo row / column, and the warm-up plane
+        const bool clear = range_clear(z0 - 1, z0 + c.tz - 1, nz, g->P[2]) &&
+                           range_clear(y0 - 1, y0 + c.ty - 1, ny, g->P[1]) &&
+                           range_clear(xb - 1, xe - 1, nx, g->P[0]);
+        std::vector<int>& v = clear ? inner : shell;
+        v.push_back(tz);
+        v.push_back(ty);
+        v.push_back(ch);
+      }
+  TRY(upload(&g->d_shell, shell, &g->bytes));
+  TRY(upload(&g->d_inner, inner, &g->bytes));
+  g->n_shell = (int)shell.size() / 3;
+  g->n_inner = (int)inner.size() / 3;
+  g->split_cfg = cfg;
+  g->split_chunk = chunk;
+  return JXF_OK;
+}
+
+// One leapfrog step on the TMA path.  CPML grids: the CPML kernel over the
+// shell blocks, then the plain kernel over the interior blocks (disjoint
+// outputs, both read the same input set).
+int launch_step(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStream_t st) {
+  p.pdl = g->use_pdl ? (PDL_WAIT_START | PDL_TRIGGER) : 0;
+  if (g->mode != MODE_CPML) {
+    p.blk_list = nullptr;
+    return launch_tma(g, cfg, chunk, p, in_set, st, -1);
+  }
+  TRY(build_split(g, cfg, chunk));
+  if (g->n_shell > 0) {
+    p.blk_list = g->d_shell;
+    TRY(launch_tma(g, cfg, chunk, p, in_set, st, g->n_shell));
+  }
+  if (g->n_inner > 0) {
+    Step3D q = p;
+    q.blk_list = g->d_inner;
+    q.probe_out = (g->n_shell > 0) ? nullptr : p.probe_out;
+    // runs beside the shell kernel (it was released after the shell kernel
+    // had waited for the previous step) and waits for it before exiting
+    if (g->use_pdl && g->n_shell > 0) q.pdl = PDL_TRIGGER | PDL_WAIT_END;
+    TRY(launch_tma(g, cfg, chunk, q, in_set, st, g->n_inner, /*plain=*/true));
+  }
   return JXF_OK;
 }
 
@@ -500,10 +594,10 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
         p.probe_out = nullptr;
         p.step = 0;
         p.err = g->d_err;
-        TRY(launch_tma(g, ci, ch, p, g->cur, st));
+        TRY(launch_step(g, ci, ch, p, g->cur, st));
         CUDA_TRY(cudaEventRecord(e0, st));
         const int reps = g->n >= (1LL << 25) ? 3 : 10;
-        for (int r = 0; r < reps; ++r) TRY(launch_tma(g, ci, ch, p, g->cur, st));
+        for (int r = 0; r < reps; ++r) TRY(launch_step(g, ci, ch, p, g->cur, st));
         CUDA_TRY(cudaEventRecord(e1, st));
         CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0;
@@ -579,6 +673,23 @@ int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out) {
     return fail(JXF_ERR_INVALID, "TMA path needs nz %% 4 == 0 and a non-periodic boundary");
   }
   g->path = (d.path == JXF_PATH_GENERIC || !tma_ok) ? JXF_PATH_GENERIC : JXF_PATH_TMA;
+  {
+    const char* e = std::getenv("JXF_PDL");
+    g->use_pdl = !(e && e[0] == '0');
+  }
+  if (g->mode == MODE_CPML && g->path == JXF_PATH_TMA) {
+    // the TMA kernel addresses psi slabs with 32-bit offsets
+    const long long P2 = 2LL * (d.pml_layers + 1);
+    const long long big = (long long)std::max(d.nx, std::max(d.ny, d.nz));
+    const long long mid = (long long)d.nx * d.ny * d.nz / big;
+    if (std::min(P2, big) * mid >= (1LL << 31) || (long long)d.ny * d.nz >= (1LL << 31)) {
+      if (d.path == JXF_PATH_TMA) {
+        delete g;
+        return fail(JXF_ERR_INVALID, "grid too large for 32-bit CPML slab offsets on the TMA path");
+      }
+      g->path = JXF_PATH_GENERIC;
+    }
+  }
 
   auto cleanup_fail = [&](int rc) {
     jxf_grid3d_destroy(g);
@@ -673,6 +784,8 @@ int jxf_grid3d_destroy(jxf_grid3d* g) {
   dfree(g->d_terms);
   dfree(g->d_entries);
   dfree(g->d_blk_ptr);
+  dfree(g->d_shell);
+  dfree(g->d_inner);
   dfree(g->d_wave);
   dfree(g->d_probe_cell);
   dfree(g->d_probe_comp);
@@ -840,7 +953,7 @@ int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stre
       set_io(g, p, g->cur, 1 - g->cur);
       p.step = g->step;
       p.probe_out = (probe_out && np > 0 && k >= 1) ? probe_out + (size_t)(k - 1) * np : nullptr;
-      TRY(launch_tma(g, g->cfg, g->x_chunk, p, g->cur, st));
+      TRY(launch_step(g, g->cfg, g->x_chunk, p, g->cur, st));
       g->cur ^= 1;
       g->step++;
     }

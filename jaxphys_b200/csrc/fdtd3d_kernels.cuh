@@ -354,10 +354,11 @@ struct TmaLayout {
   static constexpr uint32_t STAGE_TX =
       (uint32_t)(3 * EH * EW + 3 * HH * HW + (CBARR ? TY * TZ : 0)) * 4u;
   static constexpr int HN_STRIDE = round32(NH * NW);
-  // CPML: psi of the current and next plane, per thread: 12 core values per
-  // row and 4 halo values (double buffered).
-  static constexpr int PSC_FLOATS = CPML ? 2 * PSI_COUNT * RY * NT : 0;
-  static constexpr int PSH_FLOATS = CPML ? 2 * 4 * (TZ + TY) : 0;
+  // CPML: psi of the planes in flight, per thread: 12 core values per row and
+  // 4 halo values, in a ring of PSB buffers (prefetch distance PSB-1 planes).
+  static constexpr int PSB = 2;
+  static constexpr int PSC_FLOATS = CPML ? PSB * PSI_COUNT * RY * NT : 0;
+  static constexpr int PSH_FLOATS = CPML ? PSB * 4 * (TZ + TY) : 0;
   static constexpr size_t SMEM_BYTES =
       128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + 3 * (size_t)HN_STRIDE +
                              PSC_FLOATS + PSH_FLOATS);
@@ -368,6 +369,30 @@ struct TmaLayout {
   static_assert(TZ + TY <= NT, "halo pass needs TZ + TY threads");
   static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per block exceeds 227 KB");
 };
+
+// CPML component update written as a select: both the CPML and the plain
+// value are formed and the plain one is kept when neither axis of the
+// component is in its slab (the generic kernel branches on the same
+// condition, so the two paths produce identical bits).
+template <bool KAPPA>
+__device__ __forceinline__ float h_sel(float h, float a, float d1, float d2, bool on1, bool on2,
+                                       float p1, float p2, float ik1, float ik2) {
+  const float u1 = KAPPA ? fmul(ik1, d1) : d1;
+  const float u2 = KAPPA ? fmul(ik2, d2) : d2;
+  const float c = fsub(h, fmul(a, fadd(fsub(u1, u2), fsub(p1, p2))));
+  return (on1 || on2) ? c : h_plain(h, a, d1, d2);
+}
+template <bool KAPPA>
+__device__ __forceinline__ float e_sel(float e, float cb, float d1, float d2, bool on1, bool on2,
+                                       float p1, float p2, float ik1, float ik2) {
+  const float u1 = KAPPA ? fmul(ik1, d1) : d1;
+  const float u2 = KAPPA ? fmul(ik2, d2) : d2;
+  const float c = fadd(e, fmul(cb, fadd(fsub(u1, u2), fsub(p1, p2))));
+  return (on1 || on2) ? c : e_plain(e, cb, d1, d2);
+}
+__device__ __forceinline__ float pnext(bool on, float b, float c, float old, float d) {
+  return on ? psi_next(b, old, c, d) : 0.0f;
+}
 
 template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA>
 __global__ void __launch_bounds__(TZ*(TY / RY))
@@ -390,9 +415,15 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   const int tid = threadIdx.x;
   const int tx = tid % TZ;
   const int ty = tid / TZ;
-  const int z0 = blockIdx.x * TZ;
-  const int y0 = blockIdx.y * TY;
-  const int xb = blockIdx.z * p.x_chunk;
+  int tzi = blockIdx.x, tyi = blockIdx.y, ci = blockIdx.z;
+  if (p.blk_list != nullptr) {
+    tzi = p.blk_list[3 * blockIdx.x];
+    tyi = p.blk_list[3 * blockIdx.x + 1];
+    ci = p.blk_list[3 * blockIdx.x + 2];
+  }
+  const int z0 = tzi * TZ;
+  const int y0 = tyi * TY;
+  const int xb = ci * p.x_chunk;
   const int xe = min(xb + p.x_chunk, nx);
   const int qs = xb > 0 ? xb - 1 : 0;  // first plane staged
   const int qe = min(xe, nx - 1);      // last plane staged
@@ -400,8 +431,16 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   const float a = p.a;
   const int z = z0 + tx;
 
+  // Programmatic dependent launch: a step kernel waits for the previous
+  // step's grids before touching its inputs and then lets the next launch be
+  // scheduled; the plain interior kernel of a CPML step overlaps the shell
+  // kernel it depends on and only waits for it before exiting (so the next
+  // step, which waits on the interior kernel, also sees the shell's writes).
+  if (p.pdl & PDL_WAIT_START) grid_dep_wait();
+  if (p.pdl & PDL_TRIGGER) grid_dep_launch_dependents();
+
   // Probes of the input state (= after the previous step).
-  if (p.probe_out != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+  if (p.probe_out != nullptr && tzi == 0 && tyi == 0 && ci == 0) {
     for (int i = tid; i < p.n_probes; i += NT) p.probe_out[i] = p.in[p.probe_comp[i]][p.probe_cell[i]];
   }
 
@@ -436,35 +475,84 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   }
   int issued = min(STAGES, nload);  // identical in every thread
 
-  // ---- CPML: slab coordinates and coefficients of this thread's cells
-  // (fixed over the march along x)
-  int jm_r[RY];
-  int km = -1;
-  AxisCoef cz{};
-  int jm_h = -1, km_h = -1;  // halo cell slab indices
-  int yh = -1, zh = -1;      // halo cell (-1: none)
+  // ---- CPML per-thread state, fixed over the march along x.
+  // psi offsets are 32-bit: plane stride * plane + in-plane offset.
+  const int SY = CPML ? p.pml.L[1] * nz : 0;  // y-slab arrays: [nx][L1][nz]
+  const int SZ = CPML ? ny * p.pml.L[2] : 0;  // z-slab arrays: [nx][ny][L2]
+  const int SX = ny * nz;                     // x-slab arrays: [L0][ny][nz]
+  bool iny[RY], inz = false;
+  int oy[RY], oz[RY], ox[RY];
+  float ybh[RY], ych[RY], ybe[RY], yce[RY], yikh[RY], yike[RY];
+  float zbh = 1.f, zch = 0.f, zbe = 1.f, zce = 0.f, zikh = 1.f, zike = 1.f;
+  // halo cell (row y0-1 for tid < TZ, column z0-1 for TZ <= tid < TZ+TY)
+  int yh = -1, zh = -1;
+  bool inyh = false, inzh = false;
+  int oyh = 0, ozh = 0, oxh = 0;
+  float hyb = 1.f, hyc = 0.f, hyik = 1.f, hzb = 1.f, hzc = 0.f, hzik = 1.f;
   if (CPML) {
-    km = (z < nz) ? slab_map(z, nz, p.pml.P[2]) : -1;
-    if (z < nz) cz = axis_coef(p.pml, 2, z);
+    const int km = (z < nz) ? slab_map(z, nz, p.pml.P[2]) : -1;
+    inz = km >= 0;
+    if (z < nz) {
+      zbh = __ldg(p.pml.tab[2][TAB_BH] + z);
+      zch = __ldg(p.pml.tab[2][TAB_CH] + z);
+      zbe = __ldg(p.pml.tab[2][TAB_BE] + z);
+      zce = __ldg(p.pml.tab[2][TAB_CE] + z);
+      if (KAPPA) {
+        zikh = __ldg(p.pml.tab[2][TAB_IKH] + z);
+        zike = __ldg(p.pml.tab[2][TAB_IKE] + z);
+      }
+    }
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       const int y = y0 + ty + r * TYT;
-      jm_r[r] = (y < ny) ? slab_map(y, ny, p.pml.P[1]) : -1;
+      const bool valid = (y < ny) && (z < nz);
+      const int jm = (y < ny) ? slab_map(y, ny, p.pml.P[1]) : -1;
+      iny[r] = valid && jm >= 0;
+      oy[r] = jm * nz + z;
+      oz[r] = y * p.pml.L[2] + km;
+      ox[r] = y * nz + z;
+      const int yc = y < ny ? y : ny - 1;
+      ybh[r] = __ldg(p.pml.tab[1][TAB_BH] + yc);
+      ych[r] = __ldg(p.pml.tab[1][TAB_CH] + yc);
+      ybe[r] = __ldg(p.pml.tab[1][TAB_BE] + yc);
+      yce[r] = __ldg(p.pml.tab[1][TAB_CE] + yc);
+      yikh[r] = KAPPA ? __ldg(p.pml.tab[1][TAB_IKH] + yc) : 1.f;
+      yike[r] = KAPPA ? __ldg(p.pml.tab[1][TAB_IKE] + yc) : 1.f;
     }
-    if (tid < TZ) {  // row halo (y0-1, z0+tid)
+    if (tid < TZ) {
       if (y0 >= 1 && z0 + tid < nz) {
         yh = y0 - 1;
         zh = z0 + tid;
       }
-    } else if (tid < NH) {  // column halo (y0+tid-TZ, z0-1)
+    } else if (tid < NH) {
       if (z0 >= 1 && y0 + tid - TZ < ny) {
         yh = y0 + tid - TZ;
         zh = z0 - 1;
       }
     }
     if (yh >= 0) {
-      jm_h = slab_map(yh, ny, p.pml.P[1]);
-      km_h = slab_map(zh, nz, p.pml.P[2]);
+      const int jmh = slab_map(yh, ny, p.pml.P[1]);
+      const int kmh = slab_map(zh, nz, p.pml.P[2]);
+      inyh = jmh >= 0;
+      inzh = kmh >= 0;
+      oyh = jmh * nz + zh;
+      ozh = yh * p.pml.L[2] + kmh;
+      oxh = yh * nz + zh;
+      hyb = __ldg(p.pml.tab[1][TAB_BH] + yh);
+      hyc = __ldg(p.pml.tab[1][TAB_CH] + yh);
+      hzb = __ldg(p.pml.tab[2][TAB_BH] + zh);
+      hzc = __ldg(p.pml.tab[2][TAB_CH] + zh);
+      if (KAPPA) {
+        hyik = __ldg(p.pml.tab[1][TAB_IKH] + yh);
+        hzik = __ldg(p.pml.tab[2][TAB_IKH] + zh);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+      iny[r] = false;
+      oy[r] = oz[r] = ox[r] = 0;
+      ybh[r] = ych[r] = ybe[r] = yce[r] = yikh[r] = yike[r] = 0.f;
     }
   }
 #define PSC(buf, id, r) PSc[(((buf) * PSI_COUNT + (id)) * RY + (r)) * NT + tid]
@@ -474,55 +562,53 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     const int imq = slab_map(q, nx, p.pml.P[0]);
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
-      const int y = y0 + ty + r * TYT;
-      if (y < ny && z < nz) {
-        const int jm = jm_r[r];
-        if (jm >= 0) {
-          const long long iy = ys_index(q, jm, z, p.pml.L[1], nz);
-          cp_async4(&PSC(buf, PSI_HXY, r), p.pml.in[PSI_HXY] + iy);
-          cp_async4(&PSC(buf, PSI_HZY, r), p.pml.in[PSI_HZY] + iy);
-          cp_async4(&PSC(buf, PSI_EXY, r), p.pml.in[PSI_EXY] + iy);
-          cp_async4(&PSC(buf, PSI_EZY, r), p.pml.in[PSI_EZY] + iy);
-        }
-        if (km >= 0) {
-          const long long iz = zs_index(q, y, km, ny, p.pml.L[2]);
-          cp_async4(&PSC(buf, PSI_HXZ, r), p.pml.in[PSI_HXZ] + iz);
-          cp_async4(&PSC(buf, PSI_HYZ, r), p.pml.in[PSI_HYZ] + iz);
-          cp_async4(&PSC(buf, PSI_EXZ, r), p.pml.in[PSI_EXZ] + iz);
-          cp_async4(&PSC(buf, PSI_EYZ, r), p.pml.in[PSI_EYZ] + iz);
-        }
-        if (imq >= 0) {
-          const long long ix = xs_index(imq, y, z, ny, nz);
-          cp_async4(&PSC(buf, PSI_HYX, r), p.pml.in[PSI_HYX] + ix);
-          cp_async4(&PSC(buf, PSI_HZX, r), p.pml.in[PSI_HZX] + ix);
-          cp_async4(&PSC(buf, PSI_EYX, r), p.pml.in[PSI_EYX] + ix);
-          cp_async4(&PSC(buf, PSI_EZX, r), p.pml.in[PSI_EZX] + ix);
-        }
+      if (iny[r]) {
+        const int o = q * SY + oy[r];
+        cp_async4(&PSC(buf, PSI_HXY, r), p.pml.in[PSI_HXY] + o);
+        cp_async4(&PSC(buf, PSI_HZY, r), p.pml.in[PSI_HZY] + o);
+        cp_async4(&PSC(buf, PSI_EXY, r), p.pml.in[PSI_EXY] + o);
+        cp_async4(&PSC(buf, PSI_EZY, r), p.pml.in[PSI_EZY] + o);
+      }
+      const bool valid = (y0 + ty + r * TYT < ny) && (z < nz);
+      if (inz && valid) {
+        const int o = q * SZ + oz[r];
+        cp_async4(&PSC(buf, PSI_HXZ, r), p.pml.in[PSI_HXZ] + o);
+        cp_async4(&PSC(buf, PSI_HYZ, r), p.pml.in[PSI_HYZ] + o);
+        cp_async4(&PSC(buf, PSI_EXZ, r), p.pml.in[PSI_EXZ] + o);
+        cp_async4(&PSC(buf, PSI_EYZ, r), p.pml.in[PSI_EYZ] + o);
+      }
+      if (imq >= 0 && valid) {
+        const int o = imq * SX + ox[r];
+        cp_async4(&PSC(buf, PSI_HYX, r), p.pml.in[PSI_HYX] + o);
+        cp_async4(&PSC(buf, PSI_HZX, r), p.pml.in[PSI_HZX] + o);
+        cp_async4(&PSC(buf, PSI_EYX, r), p.pml.in[PSI_EYX] + o);
+        cp_async4(&PSC(buf, PSI_EZX, r), p.pml.in[PSI_EZX] + o);
       }
     }
     if (yh >= 0) {
-      if (jm_h >= 0)
-        cp_async4(&PSH(buf, 0), p.pml.in[PSI_HXY] + ys_index(q, jm_h, zh, p.pml.L[1], nz));
-      if (km_h >= 0)
-        cp_async4(&PSH(buf, 1), p.pml.in[PSI_HXZ] + zs_index(q, yh, km_h, ny, p.pml.L[2]));
+      if (inyh) cp_async4(&PSH(buf, 0), p.pml.in[PSI_HXY] + q * SY + oyh);
+      if (inzh) cp_async4(&PSH(buf, 1), p.pml.in[PSI_HXZ] + q * SZ + ozh);
       if (tid < TZ) {  // row halo: Hz needs hzx, hzy
-        if (imq >= 0)
-          cp_async4(&PSH(buf, 2), p.pml.in[PSI_HZX] + xs_index(imq, yh, zh, ny, nz));
-        if (jm_h >= 0)
-          cp_async4(&PSH(buf, 3), p.pml.in[PSI_HZY] + ys_index(q, jm_h, zh, p.pml.L[1], nz));
+        if (imq >= 0) cp_async4(&PSH(buf, 2), p.pml.in[PSI_HZX] + imq * SX + oxh);
+        if (inyh) cp_async4(&PSH(buf, 3), p.pml.in[PSI_HZY] + q * SY + oyh);
       } else {  // column halo: Hy needs hyz, hyx
-        if (km_h >= 0)
-          cp_async4(&PSH(buf, 2), p.pml.in[PSI_HYZ] + zs_index(q, yh, km_h, ny, p.pml.L[2]));
-        if (imq >= 0)
-          cp_async4(&PSH(buf, 3), p.pml.in[PSI_HYX] + xs_index(imq, yh, zh, ny, nz));
+        if (inzh) cp_async4(&PSH(buf, 2), p.pml.in[PSI_HYZ] + q * SZ + ozh);
+        if (imq >= 0) cp_async4(&PSH(buf, 3), p.pml.in[PSI_HYX] + imq * SX + oxh);
       }
     }
     cp_async_commit();
   };
-  if (CPML) issue_psi(qs, 0);
+  constexpr int PSB = L::PSB;
+  if (CPML) {
+#pragma unroll
+    for (int k = 0; k < PSB - 1; ++k) {
+      if (qs + k < xe) issue_psi(qs + k, k);
+      else cp_async_commit();
+    }
+  }
 
   // source list of this block
-  const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const int bid = (ci * p.ntiles_y + tyi) * p.ntiles_z + tzi;
   int sp = 0, se = 0;
   if (p.blk_src_ptr != nullptr) {
     sp = p.blk_src_ptr[bid];
@@ -541,11 +627,11 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
 
   for (int x = qs; x < xe; ++x) {
     const int l = x - qs;
-    const int pb = l & 1;  // psi buffer of this plane
+    const int pb = l % PSB;  // psi buffer of this plane
     if (CPML) {
-      if (x + 1 < xe) issue_psi(x + 1, pb ^ 1);
-      else cp_async_commit();  // empty group keeps the wait_group count uniform
-      cp_async_wait_prev();    // this plane's psi has landed (own copies only)
+      if (x + PSB - 1 < xe) issue_psi(x + PSB - 1, (l + PSB - 1) % PSB);
+      else cp_async_commit();            // empty group keeps the count uniform
+      cp_async_wait_pending<PSB - 1>();  // this plane's psi has landed (own copies)
     }
     const int slot = l % STAGES;
     const bool have_next = (x + 1 <= qe);
@@ -564,10 +650,19 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
 #define HN_AT(c, yy, zc) Hn[(c) * L::HN_STRIDE + (yy) * NW + (zc)]
     const bool warm = (x < xb);
     int imx = -1;
-    AxisCoef cx{};
+    float xbh = 1.f, xch = 0.f, xbe = 1.f, xce = 0.f, xikh = 1.f, xike = 1.f;
     if (CPML) {
       imx = slab_map(x, nx, p.pml.P[0]);
-      cx = axis_coef(p.pml, 0, x);
+      if (imx >= 0) {
+        xbh = __ldg(p.pml.tab[0][TAB_BH] + x);
+        xch = __ldg(p.pml.tab[0][TAB_CH] + x);
+        xbe = __ldg(p.pml.tab[0][TAB_BE] + x);
+        xce = __ldg(p.pml.tab[0][TAB_CE] + x);
+        if (KAPPA) {
+          xikh = __ldg(p.pml.tab[0][TAB_IKH] + x);
+          xike = __ldg(p.pml.tab[0][TAB_IKE] + x);
+        }
+      }
     }
     const bool inx = imx >= 0;
 
@@ -578,55 +673,48 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       const int yl = ty + r * TYT;
       const int y = y0 + yl;
       const int yy = yl + 1;
-      const bool own = !warm && (y < ny) && (z < nz);
+      const bool valid = (y < ny) && (z < nz);
+      const bool own = !warm && valid;
       const float exc = E_AT(0, yy, zz), eyc = E_AT(1, yy, zz), ezc = E_AT(2, yy, zz);
       exr[r] = exc;
       eyr[r] = eyc;
       ezr[r] = ezc;
       float hx = H_AT(0, yy, zz), hy = H_AT(1, yy, zz), hz = H_AT(2, yy, zz);
-      const bool iny = CPML && jm_r[r] >= 0, inz = CPML && km >= 0;
-      // Cells outside every slab take the plain update (identical value: psi
-      // is 0 and 1/kappa is 1 there) without touching any CPML state.
-      auto h_phase = [&](auto cpm) {
-        constexpr bool CP = decltype(cpm)::value;
-        const long long ix = CP ? xs_index(imx, y, z, ny, nz) : 0;
-        const long long iy = CP ? ys_index(x, jm_r[r], z, p.pml.L[1], nz) : 0;
-        const long long iz = CP ? zs_index(x, y, km, ny, p.pml.L[2]) : 0;
-        if (!warm && y < ny - 1 && z < nz - 1) {  // Hx: d/dy Ez - d/dz Ey
-          const float d1 = fsub(E_AT(2, yy + 1, zz), ezc), d2 = fsub(E_AT(1, yy, zz + 1), eyc);
-          if (CP)
-            hx = h_cpml<KAPPA>(
-                hx, a, d1, d2,
-                term_h_at(p.pml, 1, y, iny, PSC(pb, PSI_HXY, r), own ? p.pml.out[PSI_HXY] + iy : nullptr),
-                term_h(inz, cz, PSC(pb, PSI_HXZ, r), own ? p.pml.out[PSI_HXZ] + iz : nullptr));
-          else
-            hx = h_plain(hx, a, d1, d2);
+      const bool ux = !warm && y < ny - 1 && z < nz - 1;
+      const bool uy = x < nx - 1 && z < nz - 1 && y < ny;
+      const bool uz = x < nx - 1 && y < ny - 1 && z < nz;
+      const float dyEz = fsub(E_AT(2, yy + 1, zz), ezc), dzEy = fsub(E_AT(1, yy, zz + 1), eyc);
+      const float dzEx = fsub(E_AT(0, yy, zz + 1), exc), dxEz = fsub(EN_AT(2, yy, zz), ezc);
+      const float dxEy = fsub(EN_AT(1, yy, zz), eyc), dyEx = fsub(E_AT(0, yy + 1, zz), exc);
+      const bool cinz = inz && valid, cinx = inx && valid;
+      if (CPML && __any_sync(0xffffffffu, iny[r] || cinz || cinx)) {
+        const int oyq = x * SY + oy[r], ozq = x * SZ + oz[r], oxq = imx * SX + ox[r];
+        if (ux) {
+          const float p1 = pnext(iny[r], ybh[r], ych[r], PSC(pb, PSI_HXY, r), dyEz);
+          const float p2 = pnext(cinz, zbh, zch, PSC(pb, PSI_HXZ, r), dzEy);
+          if (own && iny[r]) p.pml.out[PSI_HXY][oyq] = p1;
+          if (own && cinz) p.pml.out[PSI_HXZ][ozq] = p2;
+          hx = h_sel<KAPPA>(hx, a, dyEz, dzEy, iny[r], cinz, p1, p2, yikh[r], zikh);
         }
-        if (x < nx - 1 && z < nz - 1 && y < ny) {  // Hy: d/dz Ex - d/dx Ez
-          const float d1 = fsub(E_AT(0, yy, zz + 1), exc), d2 = fsub(EN_AT(2, yy, zz), ezc);
-          if (CP)
-            hy = h_cpml<KAPPA>(
-                hy, a, d1, d2,
-                term_h(inz, cz, PSC(pb, PSI_HYZ, r), own ? p.pml.out[PSI_HYZ] + iz : nullptr),
-                term_h(inx, cx, PSC(pb, PSI_HYX, r), own ? p.pml.out[PSI_HYX] + ix : nullptr));
-          else
-            hy = h_plain(hy, a, d1, d2);
+        if (uy) {
+          const float p1 = pnext(cinz, zbh, zch, PSC(pb, PSI_HYZ, r), dzEx);
+          const float p2 = pnext(cinx, xbh, xch, PSC(pb, PSI_HYX, r), dxEz);
+          if (own && cinz) p.pml.out[PSI_HYZ][ozq] = p1;
+          if (own && cinx) p.pml.out[PSI_HYX][oxq] = p2;
+          hy = h_sel<KAPPA>(hy, a, dzEx, dxEz, cinz, cinx, p1, p2, zikh, xikh);
         }
-        if (x < nx - 1 && y < ny - 1 && z < nz) {  // Hz: d/dx Ey - d/dy Ex
-          const float d1 = fsub(EN_AT(1, yy, zz), eyc), d2 = fsub(E_AT(0, yy + 1, zz), exc);
-          if (CP)
-            hz = h_cpml<KAPPA>(
-                hz, a, d1, d2,
-                term_h(inx, cx, PSC(pb, PSI_HZX, r), own ? p.pml.out[PSI_HZX] + ix : nullptr),
-                term_h_at(p.pml, 1, y, iny, PSC(pb, PSI_HZY, r), own ? p.pml.out[PSI_HZY] + iy : nullptr));
-          else
-            hz = h_plain(hz, a, d1, d2);
+        if (uz) {
+          const float p1 = pnext(cinx, xbh, xch, PSC(pb, PSI_HZX, r), dxEy);
+          const float p2 = pnext(iny[r], ybh[r], ych[r], PSC(pb, PSI_HZY, r), dyEx);
+          if (own && cinx) p.pml.out[PSI_HZX][oxq] = p1;
+          if (own && iny[r]) p.pml.out[PSI_HZY][oyq] = p2;
+          hz = h_sel<KAPPA>(hz, a, dxEy, dyEx, cinx, iny[r], p1, p2, xikh, yikh[r]);
         }
-      };
-      if (CPML && (iny || inz || inx))
-        h_phase(BoolC<CPML>{});
-      else
-        h_phase(BoolC<false>{});
+      } else {
+        if (ux) hx = h_plain(hx, a, dyEz, dzEy);
+        if (uy) hy = h_plain(hy, a, dzEx, dxEz);
+        if (uz) hz = h_plain(hz, a, dxEy, dyEx);
+      }
       hxr[r] = hx;
       hyr[r] = hy;
       hzr[r] = hz;
@@ -650,16 +738,16 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
           if (zc < nz - 1) {  // y < ny-1 holds: y0 < ny
             const float d1 = fsub(E_AT(2, 1, zb), ezc), d2 = fsub(E_AT(1, 0, zb + 1), eyc);
             if (CPML)
-              hx = h_cpml<KAPPA>(hx, a, d1, d2, term_h_at(p.pml, 1, y, jm_h >= 0, PSH(pb, 0), nullptr),
-                                 term_h_at(p.pml, 2, zc, km_h >= 0, PSH(pb, 1), nullptr));
+              hx = h_sel<KAPPA>(hx, a, d1, d2, inyh, inzh, pnext(inyh, hyb, hyc, PSH(pb, 0), d1),
+                                pnext(inzh, hzb, hzc, PSH(pb, 1), d2), hyik, hzik);
             else
               hx = h_plain(hx, a, d1, d2);
           }
           if (x < nx - 1) {
             const float d1 = fsub(EN_AT(1, 0, zb), eyc), d2 = fsub(E_AT(0, 1, zb), exc);
             if (CPML)
-              hz = h_cpml<KAPPA>(hz, a, d1, d2, term_h(inx, cx, PSH(pb, 2), nullptr),
-                                 term_h_at(p.pml, 1, y, jm_h >= 0, PSH(pb, 3), nullptr));
+              hz = h_sel<KAPPA>(hz, a, d1, d2, inx, inyh, pnext(inx, xbh, xch, PSH(pb, 2), d1),
+                                pnext(inyh, hyb, hyc, PSH(pb, 3), d2), xikh, hyik);
             else
               hz = h_plain(hz, a, d1, d2);
           }
@@ -677,16 +765,16 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
           if (y < ny - 1) {  // zc < nz-1 holds: z0 < nz
             const float d1 = fsub(E_AT(2, yy + 1, 3), ezc), d2 = fsub(E_AT(1, yy, 4), eyc);
             if (CPML)
-              hx = h_cpml<KAPPA>(hx, a, d1, d2, term_h_at(p.pml, 1, y, jm_h >= 0, PSH(pb, 0), nullptr),
-                                 term_h_at(p.pml, 2, zc, km_h >= 0, PSH(pb, 1), nullptr));
+              hx = h_sel<KAPPA>(hx, a, d1, d2, inyh, inzh, pnext(inyh, hyb, hyc, PSH(pb, 0), d1),
+                                pnext(inzh, hzb, hzc, PSH(pb, 1), d2), hyik, hzik);
             else
               hx = h_plain(hx, a, d1, d2);
           }
           if (x < nx - 1) {
             const float d1 = fsub(E_AT(0, yy, 4), exc), d2 = fsub(EN_AT(2, yy, 3), ezc);
             if (CPML)
-              hy = h_cpml<KAPPA>(hy, a, d1, d2, term_h_at(p.pml, 2, zc, km_h >= 0, PSH(pb, 2), nullptr),
-                                 term_h(inx, cx, PSH(pb, 3), nullptr));
+              hy = h_sel<KAPPA>(hy, a, d1, d2, inzh, inx, pnext(inzh, hzb, hzc, PSH(pb, 2), d1),
+                                pnext(inx, xbh, xch, PSH(pb, 3), d2), hzik, xikh);
             else
               hy = h_plain(hy, a, d1, d2);
           }
@@ -713,45 +801,39 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
         float ex = exr[r], ey = eyr[r], ez = ezr[r];
         const float hxc = hxr[r], hyc = hyr[r], hzc = hzr[r];
         const float cb = CBARR ? CBs[yl * TZ + tx] : p.cb_const;
-        const bool iny = CPML && own && jm_r[r] >= 0, inz = CPML && own && km >= 0;
-        const bool inxo = own && inx;
-        auto e_phase = [&](auto cpm) {
-          constexpr bool CP = decltype(cpm)::value;
-          const long long ix = CP ? xs_index(imx, y, z, ny, nz) : 0;
-          const long long iy = CP ? ys_index(x, jm_r[r], z, p.pml.L[1], nz) : 0;
-          const long long iz = CP ? zs_index(x, y, km, ny, p.pml.L[2]) : 0;
-          if (y >= 1 && z >= 1) {  // Ex: d/dy Hz - d/dz Hy
-            const float d1 = fsub(hzc, HN_AT(2, yy - 1, zn)), d2 = fsub(hyc, HN_AT(1, yy, zn - 1));
-            if (CP)
-              ex = e_cpml<KAPPA>(ex, cb, d1, d2,
-                                 term_e_at(p.pml, 1, y, iny, PSC(pb, PSI_EXY, r), p.pml.out[PSI_EXY] + iy),
-                                 term_e(inz, cz, PSC(pb, PSI_EXZ, r), p.pml.out[PSI_EXZ] + iz));
-            else
-              ex = e_plain(ex, cb, d1, d2);
+        const bool ux = y >= 1 && z >= 1, uy = x >= 1 && z >= 1, uz = x >= 1 && y >= 1;
+        const float dyHz = fsub(hzc, HN_AT(2, yy - 1, zn)), dzHy = fsub(hyc, HN_AT(1, yy, zn - 1));
+        const float dzHx = fsub(hxc, HN_AT(0, yy, zn - 1)), dxHz = fsub(hzc, hz_prev[r]);
+        const float dxHy = fsub(hyc, hy_prev[r]), dyHx = fsub(hxc, HN_AT(0, yy - 1, zn));
+        const bool cinz = inz && own, cinx = inx && own;
+        if (CPML && __any_sync(0xffffffffu, iny[r] || cinz || cinx)) {
+          const int oyq = x * SY + oy[r], ozq = x * SZ + oz[r], oxq = imx * SX + ox[r];
+          if (ux) {
+            const float p1 = pnext(iny[r], ybe[r], yce[r], PSC(pb, PSI_EXY, r), dyHz);
+            const float p2 = pnext(cinz, zbe, zce, PSC(pb, PSI_EXZ, r), dzHy);
+            if (iny[r]) p.pml.out[PSI_EXY][oyq] = p1;
+            if (cinz) p.pml.out[PSI_EXZ][ozq] = p2;
+            ex = e_sel<KAPPA>(ex, cb, dyHz, dzHy, iny[r], cinz, p1, p2, yike[r], zike);
           }
-          if (x >= 1 && z >= 1) {  // Ey: d/dz Hx - d/dx Hz
-            const float d1 = fsub(hxc, HN_AT(0, yy, zn - 1)), d2 = fsub(hzc, hz_prev[r]);
-            if (CP)
-              ey = e_cpml<KAPPA>(ey, cb, d1, d2,
-                                 term_e(inz, cz, PSC(pb, PSI_EYZ, r), p.pml.out[PSI_EYZ] + iz),
-                                 term_e(inxo, cx, PSC(pb, PSI_EYX, r), p.pml.out[PSI_EYX] + ix));
-            else
-              ey = e_plain(ey, cb, d1, d2);
+          if (uy) {
+            const float p1 = pnext(cinz, zbe, zce, PSC(pb, PSI_EYZ, r), dzHx);
+            const float p2 = pnext(cinx, xbe, xce, PSC(pb, PSI_EYX, r), dxHz);
+            if (cinz) p.pml.out[PSI_EYZ][ozq] = p1;
+            if (cinx) p.pml.out[PSI_EYX][oxq] = p2;
+            ey = e_sel<KAPPA>(ey, cb, dzHx, dxHz, cinz, cinx, p1, p2, zike, xike);
           }
-          if (x >= 1 && y >= 1) {  // Ez: d/dx Hy - d/dy Hx
-            const float d1 = fsub(hyc, hy_prev[r]), d2 = fsub(hxc, HN_AT(0, yy - 1, zn));
-            if (CP)
-              ez = e_cpml<KAPPA>(ez, cb, d1, d2,
-                                 term_e(inxo, cx, PSC(pb, PSI_EZX, r), p.pml.out[PSI_EZX] + ix),
-                                 term_e_at(p.pml, 1, y, iny, PSC(pb, PSI_EZY, r), p.pml.out[PSI_EZY] + iy));
-            else
-              ez = e_plain(ez, cb, d1, d2);
+          if (uz) {
+            const float p1 = pnext(cinx, xbe, xce, PSC(pb, PSI_EZX, r), dxHy);
+            const float p2 = pnext(iny[r], ybe[r], yce[r], PSC(pb, PSI_EZY, r), dyHx);
+            if (cinx) p.pml.out[PSI_EZX][oxq] = p1;
+            if (iny[r]) p.pml.out[PSI_EZY][oyq] = p2;
+            ez = e_sel<KAPPA>(ez, cb, dxHy, dyHx, cinx, iny[r], p1, p2, xike, yike[r]);
           }
-        };
-        if (CPML && (iny || inz || inxo))
-          e_phase(BoolC<CPML>{});
-        else
-          e_phase(BoolC<false>{});
+        } else {
+          if (ux) ex = e_plain(ex, cb, dyHz, dzHy);
+          if (uy) ey = e_plain(ey, cb, dzHx, dxHz);
+          if (uz) ez = e_plain(ez, cb, dxHy, dyHx);
+        }
         if (MODE == MODE_ABSORB && own) {
           const float f =
               fmul(fmul(__ldg(p.damp[0] + x), __ldg(p.damp[1] + y)), __ldg(p.damp[2] + z));
@@ -827,6 +909,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     }
     __syncthreads();
   }
+  if (p.pdl & PDL_WAIT_END) grid_dep_wait();
 }
 
 }  // namespace jxf

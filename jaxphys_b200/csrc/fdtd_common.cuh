@@ -82,7 +82,23 @@ struct Step3D {
   unsigned long long wait_ns;  // bound on every mbarrier wait
   int x_chunk;
   int ntiles_y, ntiles_z;
+  // Optional compact list of blocks (tile_z, tile_y, chunk) triples; nullptr
+  // = the launch grid itself.  Used to run the shell and the interior of a
+  // CPML grid as two launches with different kernels.
+  const int* blk_list;
+  int pdl;  // PDL_* bits
 };
+
+enum PdlBits : int { PDL_WAIT_START = 1, PDL_TRIGGER = 2, PDL_WAIT_END = 4 };
+
+// griddepcontrol (programmatic dependent launch); no-ops for a grid launched
+// without the programmatic-serialization attribute.
+__device__ __forceinline__ void grid_dep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 __device__ __forceinline__ int slab_map(int i, int n, int P) {
   if (P < 0) return i;
@@ -167,8 +183,9 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) 
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
-__device__ __forceinline__ void cp_async_wait_prev() {
-  asm volatile("cp.async.wait_group 1;" ::: "memory");
+template <int N>
+__device__ __forceinline__ void cp_async_wait_pending() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
