@@ -149,6 +149,34 @@ int jxf_grid3d_check_error(jxf_grid3d* g, void* stream);
 /* Synchronise and scan the six fields for NaN/Inf (JXF_ERR_NONFINITE). */
 int jxf_grid3d_check_finite(jxf_grid3d* g, void* stream);
 
+/* Allocation-free stepping.  No counterpart in the reference (its solver
+ * allocates fresh JAX arrays on every call).  For callers that may not call
+ * cudaMalloc: code living inside another framework's device memory pool (an
+ * XLA custom call, for instance), work recorded into CUDA graphs, or hosts
+ * that forbid allocation at run time.  Advances the caller's six float32
+ * field buffers (device, C order (nx, ny, nz), Ex..Hz) by n_steps with the
+ * reference's ABSORBING or PEC update and no sources, using a fixed device
+ * scratch array inside the library (about 6 MB, held by every GPU that loads
+ * the library until exit) instead of allocations.  Limit: at most
+ * JXF_NOALLOC_MAX_CELLS cells, at most 4096 per axis, nz % 4 == 0; larger
+ * grids are rejected with JXF_ERR_INVALID.  cb: device per-cell
+ * dt/(eps0 dx eps_r) (float32) or NULL for vacuum.  The first call on a
+ * device resolves the scratch address (cudaGetSymbolAddress), so make it
+ * before any stream capture.  All calls share the scratch: calls that
+ * overlap on the GPU (other streams, other threads) race.  Synchronises
+ * `stream` before returning. */
+#define JXF_NOALLOC_MAX_CELLS 262144
+typedef struct {
+  int32_t nx, ny, nz;
+  double dx;
+  double dt;          /* <= 0 selects 0.99 dx/(c sqrt 3) */
+  int32_t boundary;   /* JXF_BND_ABSORBING or JXF_BND_PEC */
+  int32_t pml_layers;
+  int32_t device;
+} jxf_noalloc_desc;
+int jxf_grid3d_run_noalloc(const jxf_noalloc_desc* desc, float* const* fields,
+                           const float* cb, int32_t n_steps, void* stream);
+
 /* ---------------------------------------------------------------- 2D (TM) */
 
 /* Replaces EMGrid.__init__ (fdtd.py:93-113) and the set-up part of

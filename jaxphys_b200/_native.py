@@ -55,6 +55,15 @@ class Grid3DInfo(C.Structure):
     ]
 
 
+class NoAllocDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("dx", C.c_double), ("dt", C.c_double),
+        ("boundary", C.c_int32), ("pml_layers", C.c_int32),
+        ("device", C.c_int32),
+    ]
+
+
 class Grid2DDesc(C.Structure):
     _fields_ = [
         ("nx", C.c_int32), ("ny", C.c_int32),
@@ -94,6 +103,7 @@ SIGNATURES = {
     "jxf_grid3d_snapshot": (C.c_int, [_vp, _vp, _vp]),
     "jxf_grid3d_check_error": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_check_finite": (C.c_int, [_vp, _vp]),
+    "jxf_grid3d_run_noalloc": (C.c_int, [C.POINTER(NoAllocDesc), C.POINTER(_vp), _vp, _i32, _vp]),
     "jxf_grid2d_create": (C.c_int, [C.POINTER(Grid2DDesc), C.POINTER(_vp)]),
     "jxf_grid2d_destroy": (C.c_int, [_vp]),
     "jxf_grid2d_set_sources": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),

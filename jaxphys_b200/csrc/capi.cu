@@ -1358,3 +1358,161 @@ int jxf_grid2d_check_error(jxf_grid2d* g, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point
+// ---------------------------------------------------------------------------
+//
+// For callers that cannot call cudaMalloc: code that runs inside a memory
+// pool owned by another framework (for example an XLA custom call, which must
+// not grab device memory behind the pool's back), code recorded into a CUDA
+// graph, or hosts that forbid allocation once they are running.  The TMA step
+// kernel needs a second set of six field buffers to ping-pong into, plus the
+// damping tables and an error word; here they live in one fixed device array
+// that every GPU loading this library holds until the process exits.
+
+namespace {
+
+constexpr long long kNoAllocMaxCells = 262144;  // 64^3
+constexpr int kNoAllocMaxAxis = 4096;
+constexpr size_t kNoAllocFieldBytes = 6 * (size_t)kNoAllocMaxCells * sizeof(float);
+constexpr size_t kNoAllocTableBytes = 3 * (size_t)kNoAllocMaxAxis * sizeof(float);
+constexpr size_t kNoAllocBytes = kNoAllocFieldBytes + kNoAllocTableBytes + 256;
+
+// Device scratch of jxf_grid3d_run_noalloc: [6 fields][max cells] float32,
+// then [3 axes][max axis] damping factors, then 4 error words.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[128] = {};
+
+// Device address of the scratch array on `dev` (the current device).  The
+// host-side symbol is only a stand-in for the device array, so its address
+// is resolved once per device here and passed to the kernel.
+int noalloc_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= 128) return fail(JXF_ERR_INVALID, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || ptr == nullptr)
+      return fail(JXF_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = ptr;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  return JXF_OK;
+}
+
+}  // namespace
+
+extern "C" int jxf_grid3d_run_noalloc(const jxf_noalloc_desc* desc, float* const* fields,
+                                      const float* cb, int32_t n_steps, void* stream) {
+  if (!desc || !fields) return fail(JXF_ERR_INVALID, "null argument");
+  const jxf_noalloc_desc d = *desc;
+  for (int k = 0; k < 6; ++k)
+    if (!fields[k]) return fail(JXF_ERR_INVALID, "field pointer %d is null", k);
+  if (n_steps < 0) return fail(JXF_ERR_INVALID, "n_steps must be >= 0");
+  if (d.nx < 2 || d.ny < 2 || d.nz < 2)
+    return fail(JXF_ERR_INVALID, "grid must be at least 2 cells per axis");
+  if (d.nz % 4 != 0) return fail(JXF_ERR_INVALID, "nz must be a multiple of 4 (got %d)", d.nz);
+  if (d.nx > kNoAllocMaxAxis || d.ny > kNoAllocMaxAxis || d.nz > kNoAllocMaxAxis ||
+      (long long)d.nx * d.ny * d.nz > kNoAllocMaxCells)
+    return fail(JXF_ERR_INVALID,
+                "grid %dx%dx%d exceeds the allocation-free limit (%lld cells, %d per axis)", d.nx,
+                d.ny, d.nz, kNoAllocMaxCells, kNoAllocMaxAxis);
+  if (d.boundary != JXF_BND_ABSORBING && d.boundary != JXF_BND_PEC)
+    return fail(JXF_ERR_INVALID, "allocation-free steps support ABSORBING and PEC boundaries");
+  if (!(d.dx > 0)) return fail(JXF_ERR_INVALID, "dx must be positive");
+  if (d.pml_layers < 0) return fail(JXF_ERR_INVALID, "pml_layers must be >= 0");
+  if (n_steps == 0) return JXF_OK;
+  DeviceGuard dg(d.device);
+  if (!dg.ok) return fail(JXF_ERR_CUDA, "cannot select device %d", d.device);
+  unsigned char* base = nullptr;
+  TRY(noalloc_scratch(d.device, &base));
+  cudaStream_t st = (cudaStream_t)stream;
+  float* fB = reinterpret_cast<float*>(base);
+  float* tabs = reinterpret_cast<float*>(base + kNoAllocFieldBytes);
+  int* err = reinterpret_cast<int*>(base + kNoAllocFieldBytes + kNoAllocTableBytes);
+  const long long n = (long long)d.nx * d.ny * d.nz;
+  const double dt = d.dt > 0 ? d.dt : 0.99 * d.dx / (kC0 * std::sqrt(3.0));
+
+  // damping factors (ones for PEC) into the scratch tables; the error word
+  // keeps the previous call's value, so clear it
+  const int dims[3] = {d.nx, d.ny, d.nz};
+  for (int ax = 0; ax < 3; ++ax) {
+    std::vector<float> t = d.boundary == JXF_BND_ABSORBING
+                               ? damping_table(dims[ax], d.pml_layers, d.dx, dt, 3)
+                               : std::vector<float>(dims[ax], 1.0f);
+    CUDA_TRY(cudaMemcpyAsync(tabs + (size_t)ax * kNoAllocMaxAxis, t.data(), t.size() * 4,
+                             cudaMemcpyHostToDevice, st));
+  }
+  CUDA_TRY(cudaMemsetAsync(err, 0, 16, st));
+
+  const int cfg = 0;
+  const TmaConfig& c = tma_configs()[cfg];
+  const int chunk = n >= (1LL << 17) ? 16 : 8;
+  float* set[2][6];
+  for (int k = 0; k < 6; ++k) {
+    set[0][k] = fields[k];
+    set[1][k] = fB + (size_t)k * n;
+  }
+  Maps3D maps[2];
+  for (int s = 0; s < 2; ++s) {
+    for (int k = 0; k < 3; ++k) {
+      TRY(encode_map(&maps[s].e[k], set[s][k], d.nx, d.ny, d.nz, c.tz + 8, c.ty + 2));
+      TRY(encode_map(&maps[s].h[k], set[s][3 + k], d.nx, d.ny, d.nz, c.tz + 4, c.ty + 1));
+    }
+    if (cb) {
+      TRY(encode_map(&maps[s].cb, cb, d.nx, d.ny, d.nz, c.tz, c.ty));
+    } else {
+      maps[s].cb = maps[s].e[0];
+    }
+  }
+  Step3D p{};
+  p.nx = d.nx;
+  p.ny = d.ny;
+  p.nz = d.nz;
+  p.a = (float)(dt / (kMu0 * d.dx));
+  p.cb_const = (float)(dt / (kEps0 * d.dx));
+  p.cb = cb;
+  for (int ax = 0; ax < 3; ++ax) p.damp[ax] = tabs + (size_t)ax * kNoAllocMaxAxis;
+  for (int ax = 0; ax < 3; ++ax) {
+    for (int t = 0; t < TAB_COUNT; ++t) p.pml.tab[ax][t] = p.damp[ax];
+    p.pml.L[ax] = 0;
+    p.pml.P[ax] = -1;
+  }
+  p.err = err;
+  p.wait_ns = wait_limit_ns();
+  p.x_chunk = chunk;
+  p.ntiles_z = (d.nz + c.tz - 1) / c.tz;
+  p.ntiles_y = (d.ny + c.ty - 1) / c.ty;
+  TmaKernel k = c.k[0][cb ? 1 : 0];
+  {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)c.smem[0]));
+  }
+  const dim3 grid(p.ntiles_z, p.ntiles_y, (d.nx + chunk - 1) / chunk);
+  int cur = 0;
+  for (int s = 0; s < n_steps; ++s) {
+    for (int q = 0; q < 6; ++q) {
+      p.in[q] = set[cur][q];
+      p.out[q] = set[cur ^ 1][q];
+    }
+    p.step = s;
+    k<<<grid, c.threads, c.smem[0], st>>>(p, maps[cur]);
+    CUDA_TRY(cudaGetLastError());
+    cur ^= 1;
+  }
+  if (cur == 1)  // odd step count: the result sits in the scratch set
+    for (int q = 0; q < 6; ++q)
+      CUDA_TRY(cudaMemcpyAsync(fields[q], set[1][q], (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+  int h[4] = {0, 0, 0, 0};
+  CUDA_TRY(cudaMemcpyAsync(h, err, 16, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (h[0] != 0)
+    return fail(JXF_ERR_TIMEOUT, "a staged copy did not arrive within the wait limit (block %d)",
+                h[1]);
+  return JXF_OK;
+}
