@@ -51,9 +51,10 @@ WORKLOADS = {
     "c3": (512, 200, 12, "fdtd3d-512^3-cpml12-smoothnoise-eps1to12"),
 }
 
-# DRAM bytes per launch of the dominant kernel from an ncu capture of the same
-# workload (profiles/k3d_tma_cpml_128cubed.md); None until captured.
-NCU_TRAFFIC = {"c2": None, "c1": None, "c3": None}
+# DRAM bytes per leapfrog step (CPML shell launch + interior launch) from the
+# ncu capture of the same workload and launch shape
+# (profiles/k3d_tma_cpml_128cubed_bench_c2.md); None where not captured.
+NCU_TRAFFIC = {"c2": 124.9e6, "c1": None, "c3": None}
 
 
 def make_inputs(name: str, seed: int = 0):
@@ -278,7 +279,9 @@ def run_ours(args, world, rank, local, pg):
 
     # ---- roofline of the dominant kernel (the fused TMA step)
     info = g.info()
-    per_launch_ms = statistics.mean(kern_ms) / (nsteps + 1)
+    # one leapfrog step = the step launch(es) of one time step (the probe
+    # gather that ends each run is < 0.1 % of it)
+    per_launch_ms = statistics.mean(kern_ms) / nsteps
     b_cell = 52.0 + psi_bytes_per_cell(n, pml) if eps is not None else 48.0 + psi_bytes_per_cell(n, pml)
     bytes_per_launch = cells * b_cell
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
@@ -309,9 +312,9 @@ def run_ours(args, world, rank, local, pg):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": peak_kind, "bytes_per_cell_update": round(b_cell, 2),
-                     "kernel": "k3d_tma (fused H+E step, CPML)",
-                     "launch_ms": round(per_launch_ms, 5)},
-        "gpu_launches": (nsteps + 1) * args.steps,
+                     "kernel": "k3d_tma step (CPML shell launch + plain interior launch)",
+                     "ms_per_leapfrog_step": round(per_launch_ms, 5)},
+        "gpu_launches": (nsteps * g.kernels_per_step() + 1) * args.steps,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -346,7 +349,8 @@ def cpu_baseline(workload: str, budget_s: float = 10.0, steps: int | None = None
     el = time.perf_counter() - t0
     v = n ** 3 * steps / el / 1e9
     return {"value": round(v, 4), "unit": "Gcell/s", "cores": num_threads(), "kind": "port",
-            "sample": f"{wname}: leapfrog steps 7..{6 + steps} of {nsteps} (FP64, oracle/cpu_fdtd.c)",
+            "sample": f"{wname}: {steps} leapfrog steps of the same grid, source and "
+                      f"permittivity (FP64, oracle/cpu_fdtd.c, {num_threads()} threads)",
             "seconds": round(el, 2)}
 
 

@@ -82,6 +82,8 @@ typedef struct {
   int32_t path;               /* JXF_PATH_GENERIC or JXF_PATH_TMA in use  */
   int32_t tile_z, tile_y, rows_per_thread, stages, x_chunk;
   int64_t device_bytes;       /* device memory held by the handle         */
+  int32_t kernels_per_step;   /* step kernels launched per leapfrog step  */
+  int32_t shell_blocks, interior_blocks;  /* CPML region split (TMA path) */
 } jxf_grid3d_info;
 
 int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out);

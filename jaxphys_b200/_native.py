@@ -52,6 +52,8 @@ class Grid3DInfo(C.Structure):
         ("tile_z", C.c_int32), ("tile_y", C.c_int32), ("rows_per_thread", C.c_int32),
         ("stages", C.c_int32), ("x_chunk", C.c_int32),
         ("device_bytes", C.c_int64),
+        ("kernels_per_step", C.c_int32),
+        ("shell_blocks", C.c_int32), ("interior_blocks", C.c_int32),
     ]
 
 

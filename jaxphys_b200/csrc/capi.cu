@@ -573,6 +573,14 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
   }
   const char* env = std::getenv("JXF_AUTOTUNE");
   const bool enabled = !(env && env[0] == '0');
+  const char* forced = std::getenv("JXF_LAUNCH");  // "cfg,chunk": pin the launch shape
+  int fc = -1, fk = -1;
+  if (forced && std::sscanf(forced, "%d,%d", &fc, &fk) == 2 && fc >= 0 &&
+      fc < (int)tma_configs().size() && fk >= 1) {
+    g->cfg = fc;
+    g->x_chunk = fk;
+    return JXF_OK;
+  }
   if (!enabled || g->n < (1LL << 18)) {
     TRY(heuristic_tune(g));
   } else {
@@ -813,6 +821,14 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
     out->tile_z = out->tile_y = out->rows_per_thread = out->stages = out->x_chunk = 0;
   }
   out->device_bytes = g->bytes;
+  out->shell_blocks = g->n_shell;
+  out->interior_blocks = g->n_inner;
+  if (g->path == JXF_PATH_GENERIC)
+    out->kernels_per_step = 2 + (g->n_cells > 0 ? 1 : 0);
+  else if (g->mode == MODE_CPML && g->split_cfg >= 0)
+    out->kernels_per_step = (g->n_shell > 0 ? 1 : 0) + (g->n_inner > 0 ? 1 : 0);
+  else
+    out->kernels_per_step = 1;
   return JXF_OK;
 }
 

@@ -375,6 +375,10 @@ class EMGrid3D:
         nat.check(nat.load().jxf_grid3d_get_info(self._h, C.byref(inf)), "get_info")
         return {f: getattr(inf, f) for f, _ in nat.Grid3DInfo._fields_}
 
+    def kernels_per_step(self) -> int:
+        """Step kernels launched per leapfrog step (after the first step)."""
+        return int(self.info()["kernels_per_step"])
+
     def run(self, n_steps: int, record_probes: bool = True):
         """Extension: advance ``n_steps``; returns probe traces
         (n_steps, n_probes) as a device tensor (None without probes)."""
