@@ -129,6 +129,26 @@ int jxf_grid3d_set_probes(jxf_grid3d* g, int32_t n, const int64_t* cell,
  * only when the call synchronises; see jxf_grid3d_check_error). */
 int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stream);
 
+/* Adjoint (extension; the reference differentiates nothing in its FDTD,
+ * and jax.grad through EMGrid3D.simulate, fdtd3d.py:393, would keep every
+ * step).  Gradient of an objective J(probe traces) with respect to the
+ * per-cell relative permittivity, by the exact transpose of the discrete
+ * step, with sqrt(T) checkpointing.
+ *
+ * jxf_grid3d_adjoint_forward: reset, then run n_steps recording the probes
+ * into probe_out (device [n_steps][n_probes], may be NULL) and keeping a
+ * checkpoint of the full state every checkpoint_every steps (<= 0:
+ * ceil(sqrt(n_steps))).
+ * jxf_grid3d_adjoint_backward: probe_grad = dJ/d(probe_out) (device
+ * [n_steps][n_probes]); writes dJ/d(eps_r) (device float32 [nx*ny*nz]).
+ * Recomputes each segment forward from its checkpoint (one segment of H and
+ * psi_E snapshots is held) and runs the adjoint steps in reverse.  Leaves
+ * the grid at its initial (step 0) state.  Not for PERIODIC grids. */
+int jxf_grid3d_adjoint_forward(jxf_grid3d* g, int32_t n_steps, int32_t checkpoint_every,
+                               float* probe_out, void* stream);
+int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_grad, float* grad_eps,
+                                void* stream);
+
 /* Zero fields and psi, reset the step counter. */
 int jxf_grid3d_reset(jxf_grid3d* g, void* stream);
 

@@ -19,6 +19,7 @@
 
 #include "../../include/jaxphys_fdtd.h"
 #include "fdtd2d_kernels.cuh"
+#include "fdtd3d_adjoint.cuh"
 #include "fdtd3d_kernels.cuh"
 
 using namespace jxf;
@@ -282,6 +283,15 @@ struct jxf_grid3d {
   int n_shell = 0, n_inner = 0;
   int split_cfg = -1, split_chunk = -1;
   bool use_pdl = true;  // programmatic dependent launch between step kernels
+  // adjoint (sqrt(T) checkpointing): checkpoints of the full state every
+  // adj_k steps, one segment of per-step (H, psiE) snapshots, adjoint state
+  int adj_n = 0, adj_k = 0, adj_nseg = 0;
+  size_t adj_state = 0, adj_segstate = 0;  // floats per checkpoint / per snapshot
+  float* adj_ck = nullptr;
+  float* adj_sg = nullptr;
+  float* adj_l = nullptr;   // lE(3n) lH(3n) lpsi(psi) db(6n) dh(6n)
+  double* adj_g = nullptr;  // dJ/dcb
+  size_t adj_ck_cap = 0, adj_sg_cap = 0, adj_l_cap = 0, adj_g_cap = 0;
   // TMA selection
   int cfg = -1, x_chunk = 0;
   bool maps_ok = false;
@@ -794,6 +804,10 @@ int jxf_grid3d_destroy(jxf_grid3d* g) {
   dfree(g->d_blk_ptr);
   dfree(g->d_shell);
   dfree(g->d_inner);
+  dfree(g->adj_ck);
+  dfree(g->adj_sg);
+  dfree(g->adj_l);
+  dfree(g->adj_g);
   dfree(g->d_wave);
   dfree(g->d_probe_cell);
   dfree(g->d_probe_comp);
@@ -1374,6 +1388,199 @@ int jxf_grid2d_check_error(jxf_grid2d* g, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint (permittivity gradients of probe objectives)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+size_t psi_size(const jxf_grid3d* g, int id) {
+  static const int axis_of[PSI_COUNT] = {1, 2, 2, 0, 0, 1, 1, 2, 2, 0, 0, 1};
+  const int ax = axis_of[id];
+  if (g->mode != MODE_CPML) return 0;
+  if (ax == 0) return (size_t)g->L[0] * g->d.ny * g->d.nz;
+  if (ax == 1) return (size_t)g->d.nx * g->L[1] * g->d.nz;
+  return (size_t)g->d.nx * g->d.ny * g->L[2];
+}
+
+template <class T>
+int ensure_buf(T** p, size_t* cap, size_t count, int64_t* tally) {
+  if (*cap >= count && *p) return JXF_OK;
+  dfree(*p);
+  *cap = 0;
+  TRY(dmalloc(p, count, tally));
+  *cap = count;
+  return JXF_OK;
+}
+
+// copy the current state (fields + psi) to / from one checkpoint slot
+int ckpt_copy(jxf_grid3d* g, float* slot, bool save, cudaStream_t st) {
+  const size_t n = (size_t)g->n;
+  size_t off = 0;
+  for (int k = 0; k < 6; ++k) {
+    float* f = g->f[g->cur][k];
+    CUDA_TRY(cudaMemcpyAsync(save ? slot + off : f, save ? f : slot + off, n * 4,
+                             cudaMemcpyDeviceToDevice, st));
+    off += n;
+  }
+  for (int k = 0; k < PSI_COUNT; ++k) {
+    const size_t sz = psi_size(g, k);
+    if (!sz) continue;
+    float* q = g->psi[g->cur][k];
+    CUDA_TRY(cudaMemcpyAsync(save ? slot + off : q, save ? q : slot + off, sz * 4,
+                             cudaMemcpyDeviceToDevice, st));
+    off += sz;
+  }
+  return JXF_OK;
+}
+
+}  // namespace
+
+extern "C" int jxf_grid3d_adjoint_forward(jxf_grid3d* g, int32_t n_steps,
+                                          int32_t checkpoint_every, float* probe_out,
+                                          void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (n_steps < 1) return fail(JXF_ERR_INVALID, "n_steps must be >= 1");
+  if (g->mode == MODE_PERIODIC)
+    return fail(JXF_ERR_INVALID, "the adjoint supports ABSORBING, PEC and CPML boundaries");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int K = checkpoint_every > 0 ? checkpoint_every
+                                     : std::max(1, (int)std::ceil(std::sqrt((double)n_steps)));
+  const int nseg = (n_steps + K - 1) / K;
+  size_t state = 6 * (size_t)g->n, segstate = 3 * (size_t)g->n;
+  for (int k = 0; k < PSI_COUNT; ++k) state += psi_size(g, k);
+  for (int k = PSI_EXY; k < PSI_COUNT; ++k) segstate += psi_size(g, k);
+  TRY(ensure_buf(&g->adj_ck, &g->adj_ck_cap, state * nseg, &g->bytes));
+  TRY(jxf_grid3d_reset(g, stream));
+  const int np = g->n_probes;
+  for (int s = 0; s < nseg; ++s) {
+    const int start = s * K, len = std::min(K, n_steps - start);
+    TRY(ckpt_copy(g, g->adj_ck + (size_t)s * state, true, st));
+    TRY(jxf_grid3d_step(g, len, probe_out ? probe_out + (size_t)start * np : nullptr, stream));
+  }
+  g->adj_n = n_steps;
+  g->adj_k = K;
+  g->adj_nseg = nseg;
+  g->adj_state = state;
+  g->adj_segstate = segstate;
+  return JXF_OK;
+}
+
+extern "C" int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_grad,
+                                           float* grad_eps, void* stream) {
+  if (!g || !grad_eps) return fail(JXF_ERR_INVALID, "null argument");
+  if (g->adj_n < 1) return fail(JXF_ERR_INVALID, "call jxf_grid3d_adjoint_forward first");
+  if (g->n_probes > 0 && !probe_grad) return fail(JXF_ERR_INVALID, "probe_grad is null");
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)g->n;
+  const int K = g->adj_k, N = g->adj_n;
+  size_t psi_tot = 0;
+  for (int k = 0; k < PSI_COUNT; ++k) psi_tot += psi_size(g, k);
+  TRY(ensure_buf(&g->adj_sg, &g->adj_sg_cap, g->adj_segstate * K, &g->bytes));
+  TRY(ensure_buf(&g->adj_l, &g->adj_l_cap, 18 * n + psi_tot, &g->bytes));
+  TRY(ensure_buf(&g->adj_g, &g->adj_g_cap, n, &g->bytes));
+  CUDA_TRY(cudaMemsetAsync(g->adj_l, 0, (18 * n + psi_tot) * 4, st));
+  CUDA_TRY(cudaMemsetAsync(g->adj_g, 0, n * 8, st));
+
+  Adj3D a{};
+  a.nx = g->d.nx;
+  a.ny = g->d.ny;
+  a.nz = g->d.nz;
+  a.a = (float)g->coef_h;
+  a.cb_const = (float)g->coef_e;
+  a.cb = g->cb;
+  for (int ax = 0; ax < 3; ++ax) {
+    a.damp[ax] = g->damp[ax];
+    for (int t = 0; t < TAB_COUNT; ++t) a.pml.tab[ax][t] = g->tab[ax][t];
+    a.pml.L[ax] = g->L[ax];
+    a.pml.P[ax] = g->P[ax];
+  }
+  float* lp = g->adj_l;
+  Lam6 lam;
+  for (int c = 0; c < 3; ++c) {
+    a.lE[c] = lp + c * n;
+    a.lH[c] = lp + (3 + c) * n;
+    lam.f[c] = a.lE[c];
+    lam.f[3 + c] = a.lH[c];
+  }
+  {
+    size_t off = 6 * n;
+    for (int k = 0; k < PSI_COUNT; ++k) {
+      a.lpsi[k] = psi_size(g, k) ? lp + off : nullptr;
+      off += psi_size(g, k);
+    }
+    for (int k = 0; k < 6; ++k) {
+      a.db[k] = lp + off + k * n;
+      a.dh[k] = lp + off + (6 + k) * n;
+    }
+  }
+  a.gcb = g->adj_g;
+  const int threads = 256;
+  const int blocks = (int)std::min<long long>(((long long)n + threads - 1) / threads, 148LL * 16);
+  const int np = g->n_probes;
+
+  for (int s = g->adj_nseg - 1; s >= 0; --s) {
+    const int start = s * K, len = std::min(K, N - start);
+    // recompute the segment, keeping (H, psiE) after every step
+    TRY(ckpt_copy(g, g->adj_ck + (size_t)s * g->adj_state, false, st));
+    g->step = start;
+    for (int k = 0; k < len; ++k) {
+      TRY(jxf_grid3d_step(g, 1, nullptr, stream));
+      float* slot = g->adj_sg + (size_t)k * g->adj_segstate;
+      size_t off = 0;
+      for (int c = 0; c < 3; ++c) {
+        CUDA_TRY(cudaMemcpyAsync(slot + off, g->f[g->cur][3 + c], n * 4,
+                                 cudaMemcpyDeviceToDevice, st));
+        off += n;
+      }
+      for (int q = PSI_EXY; q < PSI_COUNT; ++q) {
+        const size_t sz = psi_size(g, q);
+        if (!sz) continue;
+        CUDA_TRY(cudaMemcpyAsync(slot + off, g->psi[g->cur][q], sz * 4, cudaMemcpyDeviceToDevice,
+                                 st));
+        off += sz;
+      }
+    }
+    // adjoint steps, last to first
+    for (int k = len - 1; k >= 0; --k) {
+      const int step_n = start + k;
+      if (np > 0) {
+        k3a_seed<<<1, 32, 0, st>>>(lam, g->d_probe_cell, g->d_probe_comp, np,
+                                   probe_grad + (size_t)step_n * np);
+      }
+      const float* slot = g->adj_sg + (size_t)k * g->adj_segstate;
+      size_t off = 0;
+      for (int c = 0; c < 3; ++c) {
+        a.fh[c] = slot + off;
+        off += n;
+      }
+      for (int q = PSI_EXY; q < PSI_COUNT; ++q) {
+        const size_t sz = psi_size(g, q);
+        a.fpsiE[q - PSI_EXY] = sz ? slot + off : nullptr;
+        off += sz;
+      }
+      if (g->mode == MODE_CPML) {
+        k3a_e<MODE_CPML><<<blocks, threads, 0, st>>>(a);
+        k3a_h<MODE_CPML><<<blocks, threads, 0, st>>>(a);
+      } else {
+        k3a_e<MODE_ABSORB><<<blocks, threads, 0, st>>>(a);
+        k3a_h<MODE_ABSORB><<<blocks, threads, 0, st>>>(a);
+      }
+      k3a_e2<<<blocks, threads, 0, st>>>(a);
+      CUDA_TRY(cudaGetLastError());
+    }
+  }
+  k3a_finish<<<blocks, threads, 0, st>>>(g->adj_g, g->cb, (float)g->coef_e, g->coef_e, grad_eps,
+                                         (long long)n);
+  CUDA_TRY(cudaGetLastError());
+  // leave the grid at its initial state
+  TRY(ckpt_copy(g, g->adj_ck, false, st));
+  g->step = 0;
+  return JXF_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free entry point

@@ -403,6 +403,38 @@ class EMGrid3D:
                                              nat.stream_handle()), "jxf_grid3d_step")
         return out
 
+    # ------------------------------------------------------------- adjoint
+    def adjoint_forward(self, n_steps: int, checkpoint_every: int | None = None):
+        """Extension: reset, run ``n_steps`` keeping sqrt(T) checkpoints for
+        :meth:`adjoint_backward`; returns the probe traces (n_steps, P)."""
+        import torch
+
+        if self._h is None:
+            self.prepare(self._dt, self._t_start)
+        elif self._dirty:
+            self._upload_config()
+        if self._sources:
+            self._ensure_waves(int(n_steps))
+        out = torch.empty((int(n_steps), len(self._probes)), dtype=torch.float32,
+                          device=f"cuda:{self._h_key[1]}")
+        nat.check(nat.load().jxf_grid3d_adjoint_forward(
+            self._h, int(n_steps), int(checkpoint_every or 0),
+            out.data_ptr() if self._probes else None, nat.stream_handle()),
+            "jxf_grid3d_adjoint_forward")
+        return out
+
+    def adjoint_backward(self, probe_grad):
+        """Extension: dJ/d(eps_r) (device tensor of the grid shape) for
+        ``probe_grad`` = dJ/d(probe traces) of the last adjoint_forward."""
+        import torch
+
+        g = probe_grad.detach().to(torch.float32).contiguous()
+        out = torch.empty(self.size, dtype=torch.float32, device=f"cuda:{self._h_key[1]}")
+        nat.check(nat.load().jxf_grid3d_adjoint_backward(self._h, g.data_ptr(), out.data_ptr(),
+                                                         nat.stream_handle()),
+                  "jxf_grid3d_adjoint_backward")
+        return out
+
     def step(self, n: int = 1) -> None:
         """Extension: advance ``n`` steps without probe recording."""
         self.run(n, record_probes=False)

@@ -80,9 +80,15 @@ class Oracle3DC:
         nx, ny, nz = self.shape
         n_src = len(self.src)
         vals = np.zeros((max(n_steps, 1), max(n_src, 1)))
+        cache = {}
         for k, s in enumerate(self.src):
-            vals[:n_steps, k] = rn.waveform_values(s, n_steps, self.dt, self.t_start,
-                                                   step0=self.step_idx)
+            key = (s.get("kind", "sine"), s.get("frequency"), s.get("width_steps"),
+                   s.get("delay_steps"))
+            if key not in cache:  # unit-amplitude samples of each distinct waveform
+                unit = dict(s, amplitude=1.0)
+                cache[key] = rn.waveform_values(unit, n_steps, self.dt, self.t_start,
+                                                step0=self.step_idx)
+            vals[:n_steps, k] = float(s.get("amplitude", 1.0)) * cache[key]
         vals = np.ascontiguousarray(vals)
         probes = np.zeros((max(n_steps, 1), max(len(self.probe_cell), 1)))
         tab_p = _ptr_array(self.tabs) if self.tabs is not None else None
