@@ -149,6 +149,24 @@ int jxf_grid3d_adjoint_forward(jxf_grid3d* g, int32_t n_steps, int32_t checkpoin
 int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_grad, float* grad_eps,
                                 void* stream);
 
+/* Decomposition of one grid along x over several processes (one per GPU;
+ * the reference runs a single device).  jxf_grid3d_create_slab makes the
+ * handle of global planes [x0, x1) of the grid `desc`, stored with one ghost
+ * plane on each side (local plane 0 = global x0-1, local plane x1-x0+1 =
+ * global x1).  A step is: fill local plane x1-x0+1 with Ey, Ez of global
+ * plane x1 (the next rank's first plane), jxf_grid3d_half_step(H); fill
+ * local plane 0 with Hy, Hz of global plane x0-1 (the previous rank's last
+ * plane), jxf_grid3d_half_step(E) -- which also applies this rank's sources
+ * and records its probes into probe_row.  Sources and probes take LOCAL cell
+ * indices.  jxf_grid3d_plane copies one plane of one component between the
+ * grid and a device buffer (to_buf != 0: grid -> buffer).  PERIODIC grids are
+ * not decomposed. */
+int jxf_grid3d_create_slab(const jxf_grid3d_desc* desc, int32_t x0, int32_t x1,
+                           jxf_grid3d** out);
+int jxf_grid3d_half_step(jxf_grid3d* g, int32_t half, float* probe_row, void* stream);
+int jxf_grid3d_plane(jxf_grid3d* g, int32_t comp, int32_t plane, float* buf, int32_t to_buf,
+                     void* stream);
+
 /* Zero fields and psi, reset the step counter. */
 int jxf_grid3d_reset(jxf_grid3d* g, void* stream);
 

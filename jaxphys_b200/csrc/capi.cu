@@ -243,6 +243,11 @@ std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
 struct jxf_grid3d {
   jxf_grid3d_desc d{};
   int mode = MODE_ABSORB;   // kernel mode: ABSORB (also PEC with unit tables), PERIODIC, CPML
+  // x-slab of a decomposed grid: local plane x is global plane x + gx0 of a
+  // grid with gnx planes; planes [x_lo, x_hi) are owned, the two outer
+  // planes are ghost copies of the neighbouring ranks' planes
+  int gx0 = 0, gnx = 0, x_lo = 0, x_hi = 0;
+  bool slab = false;
   bool kappa = false;       // CPML with kappa_max > 1 (1/kappa factors are not all 1)
   int path = JXF_PATH_GENERIC;
   double dt = 0, coef_h = 0, coef_e = 0;
@@ -433,6 +438,10 @@ Step3D base_params(jxf_grid3d* g) {
   p.probe_comp = g->d_probe_comp;
   p.err = g->d_err;
   p.wait_ns = wait_limit_ns();
+  p.gx0 = g->gx0;
+  p.gnx = g->gnx;
+  p.x_lo = g->x_lo;
+  p.x_hi = g->x_hi;
   return p;
 }
 
@@ -657,10 +666,31 @@ const char* jxf_last_error(void) { return g_last_error.c_str(); }
 
 int jxf_version(void) { return 100; }
 
+static int create3d(const jxf_grid3d_desc& d, int gnx, int gx0, int x_lo, int x_hi, bool slab,
+                    jxf_grid3d** out);
+
 int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out) {
   if (!desc || !out) return fail(JXF_ERR_INVALID, "null argument");
   *out = nullptr;
-  const jxf_grid3d_desc d = *desc;
+  return create3d(*desc, desc->nx, 0, 0, desc->nx, false, out);
+}
+
+int jxf_grid3d_create_slab(const jxf_grid3d_desc* desc, int32_t x0, int32_t x1,
+                           jxf_grid3d** out) {
+  if (!desc || !out) return fail(JXF_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (x0 < 0 || x1 > desc->nx || x1 - x0 < 1)
+    return fail(JXF_ERR_INVALID, "slab [%d, %d) outside the grid's %d planes", x0, x1, desc->nx);
+  if (desc->boundary == JXF_BND_PERIODIC)
+    return fail(JXF_ERR_INVALID, "x-slab decomposition does not support PERIODIC boundaries");
+  jxf_grid3d_desc d = *desc;
+  d.nx = x1 - x0 + 2;  // owned planes plus one ghost plane on each side
+  d.path = JXF_PATH_GENERIC;
+  return create3d(d, desc->nx, x0 - 1, 1, x1 - x0 + 1, true, out);
+}
+
+static int create3d(const jxf_grid3d_desc& d, int gnx, int gx0, int x_lo, int x_hi, bool slab,
+                    jxf_grid3d** out) {
   if (d.nx < 2 || d.ny < 2 || d.nz < 2)
     return fail(JXF_ERR_INVALID, "grid must be at least 2 cells per axis, got %dx%dx%d", d.nx, d.ny,
                 d.nz);
@@ -679,6 +709,11 @@ int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out) {
   jxf_grid3d* g = new jxf_grid3d();
   g->d = d;
   g->n = (long long)d.nx * d.ny * d.nz;
+  g->gnx = gnx;
+  g->gx0 = gx0;
+  g->x_lo = x_lo;
+  g->x_hi = x_hi;
+  g->slab = slab;
   g->dt = d.dt > 0 ? d.dt : 0.99 * d.dx / (kC0 * std::sqrt(3.0));  // fdtd3d.py:190-192
   g->coef_h = g->dt / (kMu0 * d.dx);                                 // fdtd3d.py:223
   g->coef_e = g->dt / (kEps0 * d.dx);                                // fdtd3d.py:224
@@ -723,7 +758,8 @@ int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out) {
   if (g->path == JXF_PATH_GENERIC)
     for (int k = 0; k < 6; ++k) g->f[1][k] = g->f[0][k];
 
-  const int dims[3] = {d.nx, d.ny, d.nz};
+  // coefficient tables along x cover the whole (global) axis
+  const int dims[3] = {gnx, d.ny, d.nz};
   // damping tables (ones for PEC / CPML / PERIODIC)
   for (int ax = 0; ax < 3; ++ax) {
     std::vector<float> t = (d.boundary == JXF_BND_ABSORBING)
@@ -960,6 +996,8 @@ static int gather_probes(jxf_grid3d* g, int set, float* out, cudaStream_t st) {
 
 int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stream) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (g->slab)
+    return fail(JXF_ERR_INVALID, "x-slab grids advance with jxf_grid3d_half_step (ghost exchange)");
   if (n_steps < 0) return fail(JXF_ERR_INVALID, "n_steps must be >= 0");
   if (n_steps == 0) return JXF_OK;
   if (!g->src_cell.empty()) {
@@ -1020,6 +1058,61 @@ int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stre
       g->step++;
     }
   }
+  return JXF_OK;
+}
+
+int jxf_grid3d_half_step(jxf_grid3d* g, int32_t half, float* probe_row, void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (!g->slab) return fail(JXF_ERR_INVALID, "half steps are for x-slab grids");
+  if (half != 0 && half != 1) return fail(JXF_ERR_INVALID, "half must be 0 (H) or 1 (E)");
+  if (half == 1 && !g->src_cell.empty()) {
+    int max_w = 0;
+    for (int w : g->src_wave) max_w = std::max(max_w, w);
+    if (max_w >= g->n_waves || g->step + 1 > g->wave_len)
+      return fail(JXF_ERR_INVALID, "waveform table does not cover step %lld", g->step);
+  }
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  Step3D p = base_params(g);
+  set_io(g, p, 0, 0);
+  p.step = g->step;
+  const int threads = 256;
+  const long long owned = (long long)(g->x_hi - g->x_lo) * g->d.ny * g->d.nz;
+  const int blocks = (int)std::min<long long>((owned + threads - 1) / threads, 148LL * 16);
+  if (half == 0) {
+    if (g->mode == MODE_CPML)
+      jxf::k3d_generic_h<MODE_CPML><<<blocks, threads, 0, st>>>(p);
+    else
+      jxf::k3d_generic_h<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+    CUDA_TRY(cudaGetLastError());
+    return JXF_OK;
+  }
+  if (g->mode == MODE_CPML)
+    jxf::k3d_generic_e<MODE_CPML><<<blocks, threads, 0, st>>>(p);
+  else
+    jxf::k3d_generic_e<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+  CUDA_TRY(cudaGetLastError());
+  if (g->n_cells > 0) {
+    k3d_sources<<<(g->n_cells + 127) / 128, 128, 0, st>>>(g->f[0][0], g->f[0][1], g->f[0][2],
+                                                           g->d_cells, g->n_cells, g->d_terms,
+                                                           g->d_wave, g->wave_len, g->step);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (probe_row && g->n_probes > 0) TRY(gather_probes(g, 0, probe_row, st));
+  g->step++;
+  return JXF_OK;
+}
+
+int jxf_grid3d_plane(jxf_grid3d* g, int32_t comp, int32_t plane, float* buf, int32_t to_buf,
+                     void* stream) {
+  if (!g || !buf) return fail(JXF_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 5) return fail(JXF_ERR_INVALID, "comp must be 0..5");
+  if (plane < 0 || plane >= g->d.nx) return fail(JXF_ERR_INVALID, "plane %d out of range", plane);
+  DeviceGuard dg(g->d.device);
+  const size_t pl = (size_t)g->d.ny * g->d.nz;
+  float* f = g->f[g->cur][comp] + (size_t)plane * pl;
+  CUDA_TRY(cudaMemcpyAsync(to_buf ? buf : f, to_buf ? f : buf, pl * 4, cudaMemcpyDeviceToDevice,
+                           (cudaStream_t)stream));
   return JXF_OK;
 }
 
@@ -1442,6 +1535,7 @@ extern "C" int jxf_grid3d_adjoint_forward(jxf_grid3d* g, int32_t n_steps,
                                           void* stream) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
   if (n_steps < 1) return fail(JXF_ERR_INVALID, "n_steps must be >= 1");
+  if (g->slab) return fail(JXF_ERR_INVALID, "the adjoint runs on whole grids, not x-slabs");
   if (g->mode == MODE_PERIODIC)
     return fail(JXF_ERR_INVALID, "the adjoint supports ABSORBING, PEC and CPML boundaries");
   DeviceGuard dg(g->d.device);

@@ -154,17 +154,21 @@ __device__ __forceinline__ PsiTerm g_term(const CpmlDev& P, int id, bool on, flo
 template <int MODE>
 __global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Step3D p) {
   const int nx = p.nx, ny = p.ny, nz = p.nz;
-  const long long n = (long long)nx * ny * nz;
+  const long long plane = (long long)ny * nz;
+  const long long n = (long long)(p.x_hi - p.x_lo) * plane;  // owned cells
+  const long long base = (long long)p.x_lo * plane;
   const float a = p.a;
   const float* ex = p.in[0];
   const float* ey = p.in[1];
   const float* ez = p.in[2];
-  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
-       idx += (long long)gridDim.x * blockDim.x) {
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long idx = base + k;
     const int z = (int)(idx % nz);
     const long long t = idx / nz;
     const int y = (int)(t % ny);
     const int x = (int)(t / ny);
+    const int xg = x + p.gx0;  // global plane
     long long ixp, iyp, izp;  // neighbours at +1
     bool ux, uy, uz;          // Hx, Hy, Hz updated here
     if (MODE == MODE_PERIODIC) {
@@ -177,17 +181,17 @@ __global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Ste
       iyp = idx + nz;
       izp = idx + 1;
       ux = (y < ny - 1) && (z < nz - 1);
-      uy = (x < nx - 1) && (z < nz - 1);
-      uz = (x < nx - 1) && (y < ny - 1);
+      uy = (xg < p.gnx - 1) && (z < nz - 1);
+      uz = (xg < p.gnx - 1) && (y < ny - 1);
     }
     const float exc = ex[idx], eyc = ey[idx], ezc = ez[idx];
     int im = -1, jm = -1, km = -1;
     AxisCoef cx{}, cy{}, cz{};
     if (MODE == MODE_CPML) {
-      im = slab_map(x, nx, p.pml.P[0]);
+      im = slab_map(xg, p.gnx, p.pml.P[0]);
       jm = slab_map(y, ny, p.pml.P[1]);
       km = slab_map(z, nz, p.pml.P[2]);
-      cx = axis_coef(p.pml, 0, x);
+      cx = axis_coef(p.pml, 0, xg);
       cy = axis_coef(p.pml, 1, y);
       cz = axis_coef(p.pml, 2, z);
     }
@@ -227,16 +231,20 @@ __global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Ste
 template <int MODE>
 __global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Step3D p) {
   const int nx = p.nx, ny = p.ny, nz = p.nz;
-  const long long n = (long long)nx * ny * nz;
+  const long long plane = (long long)ny * nz;
+  const long long n = (long long)(p.x_hi - p.x_lo) * plane;  // owned cells
+  const long long base = (long long)p.x_lo * plane;
   const float* hx = p.out[3];  // H already advanced (in place)
   const float* hy = p.out[4];
   const float* hz = p.out[5];
-  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
-       idx += (long long)gridDim.x * blockDim.x) {
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long idx = base + k;
     const int z = (int)(idx % nz);
     const long long t = idx / nz;
     const int y = (int)(t % ny);
     const int x = (int)(t / ny);
+    const int xg = x + p.gx0;  // global plane
     long long ixm, iym, izm;
     bool ux, uy, uz;
     if (MODE == MODE_PERIODIC) {
@@ -249,8 +257,8 @@ __global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Ste
       iym = idx - nz;
       izm = idx - 1;
       ux = (y >= 1) && (z >= 1);
-      uy = (x >= 1) && (z >= 1);
-      uz = (x >= 1) && (y >= 1);
+      uy = (xg >= 1) && (z >= 1);
+      uz = (xg >= 1) && (y >= 1);
     }
     const float cb = p.cb ? p.cb[idx] : p.cb_const;
     const float hxc = hx[idx], hyc = hy[idx], hzc = hz[idx];
@@ -258,10 +266,10 @@ __global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Ste
     int im = -1, jm = -1, km = -1;
     AxisCoef cx{}, cy{}, cz{};
     if (MODE == MODE_CPML) {
-      im = slab_map(x, nx, p.pml.P[0]);
+      im = slab_map(xg, p.gnx, p.pml.P[0]);
       jm = slab_map(y, ny, p.pml.P[1]);
       km = slab_map(z, nz, p.pml.P[2]);
-      cx = axis_coef(p.pml, 0, x);
+      cx = axis_coef(p.pml, 0, xg);
       cy = axis_coef(p.pml, 1, y);
       cz = axis_coef(p.pml, 2, z);
     }
@@ -290,7 +298,7 @@ __global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Ste
                : e_plain(ez, cb, d1, d2);
     }
     if (MODE == MODE_ABSORB) {
-      const float f = fmul(fmul(__ldg(p.damp[0] + x), __ldg(p.damp[1] + y)), __ldg(p.damp[2] + z));
+      const float f = fmul(fmul(__ldg(p.damp[0] + xg), __ldg(p.damp[1] + y)), __ldg(p.damp[2] + z));
       ex = fmul(ex, f);
       ey = fmul(ey, f);
       ez = fmul(ez, f);

@@ -87,6 +87,10 @@ struct Step3D {
   // CPML grid as two launches with different kernels.
   const int* blk_list;
   int pdl;  // PDL_* bits
+  // x-slab of a decomposed grid (generic kernels): local planes [x_lo, x_hi)
+  // are updated, local plane x is global plane x + gx0 of a grid of gnx
+  // planes; planes outside the range are ghost copies of neighbouring ranks.
+  int gx0, gnx, x_lo, x_hi;
 };
 
 enum PdlBits : int { PDL_WAIT_START = 1, PDL_TRIGGER = 2, PDL_WAIT_END = 4 };

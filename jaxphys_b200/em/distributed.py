@@ -1,0 +1,318 @@
+"""One 3D grid decomposed along x over several processes (one per GPU).
+
+The reference runs on one device.  For grids larger than one GPU, this
+module splits the x axis (the slowest C-order axis, so each part is
+contiguous) into slabs, one per rank of a ``torch.distributed`` process
+group.  Each rank stores its planes plus one ghost plane on each side and
+advances them with the generic CUDA kernels of ``jaxphys_b200/csrc`` (entry
+points ``jxf_grid3d_create_slab`` / ``jxf_grid3d_half_step`` /
+``jxf_grid3d_plane``).  A leapfrog step needs two exchanges with the
+neighbouring ranks, both of two tangential components of one plane:
+
+* before the H half-step, Ey and Ez of the next rank's first plane (H at the
+  last owned plane differences E at x+1);
+* before the E half-step, Hy and Hz of the previous rank's last plane (E at
+  the first owned plane differences H at x-1).
+
+CPML psi state and the material stay local.  Point-to-point transfers go
+through the group's backend (NCCL over NVLink between GPUs; gloo through host
+memory).  Probe traces are all-reduced so every rank returns the full trace.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .. import _native as nat
+from ..exceptions import ConfigurationError
+from .fdtd3d import _BOUNDARY, COMPONENTS, CPMLSpec, PointSource3D, _POL
+from . import sources as wf
+
+
+def slab_ranges(nx: int, world: int) -> list[tuple[int, int]]:
+    """Contiguous, balanced split of ``nx`` planes into ``world`` ranges."""
+    if world < 1 or nx < world:
+        raise ConfigurationError(f"cannot split {nx} planes over {world} ranks")
+    base, extra = divmod(nx, world)
+    out, x = [], 0
+    for r in range(world):
+        n = base + (1 if r < extra else 0)
+        out.append((x, x + n))
+        x += n
+    return out
+
+
+class CudaSlabStepper:
+    """Local part of the grid on this rank's GPU (the product path)."""
+
+    def __init__(self, size, x0, x1, dx, dt, boundary, pml_layers, cpml: CPMLSpec, device: int):
+        import torch
+
+        self.torch = torch
+        self.dev = torch.device(f"cuda:{device}")
+        nx, ny, nz = size
+        self.ny, self.nz = ny, nz
+        d = nat.Grid3DDesc(nx=nx, ny=ny, nz=nz, dx=float(dx), dt=float(dt), boundary=boundary,
+                           pml_layers=int(pml_layers), cpml_order=float(cpml.order),
+                           cpml_r0=float(cpml.r0), cpml_kappa_max=float(cpml.kappa_max),
+                           cpml_alpha_max=float(cpml.alpha_max), path=nat.PATH_GENERIC,
+                           device=int(device))
+        h = C.c_void_p()
+        lib = nat.load()
+        nat.check(lib.jxf_grid3d_create_slab(C.byref(d), int(x0), int(x1), C.byref(h)),
+                  "jxf_grid3d_create_slab")
+        self.h = h
+        self.lib = lib
+        self.device = self.dev
+        self.dtype = torch.float32
+
+    def close(self):
+        if self.h is not None:
+            self.lib.jxf_grid3d_destroy(self.h)
+            self.h = None
+
+    def set_eps(self, eps_local: np.ndarray):
+        e = np.ascontiguousarray(eps_local, dtype=np.float64)
+        nat.check(self.lib.jxf_grid3d_set_eps_host(self.h, e.ctypes.data), "set_eps")
+
+    def set_sources(self, cell, comp, amp, row):
+        nat.check(self.lib.jxf_grid3d_set_sources(self.h, len(cell), cell.ctypes.data,
+                                                  comp.ctypes.data, amp.ctypes.data,
+                                                  row.ctypes.data), "set_sources")
+
+    def set_waveforms(self, table: np.ndarray):
+        nat.check(self.lib.jxf_grid3d_set_waveforms(self.h, table.shape[0], table.shape[1],
+                                                    table.ctypes.data), "set_waveforms")
+        self._table = table
+
+    def set_probes(self, cell, comp):
+        nat.check(self.lib.jxf_grid3d_set_probes(self.h, len(cell), cell.ctypes.data,
+                                                 comp.ctypes.data), "set_probes")
+
+    def reset(self):
+        nat.check(self.lib.jxf_grid3d_reset(self.h, nat.stream_handle()), "reset")
+
+    def get_plane(self, comp: int, plane: int):
+        t = self.torch.empty((self.ny, self.nz), dtype=self.torch.float32, device=self.dev)
+        nat.check(self.lib.jxf_grid3d_plane(self.h, comp, plane, t.data_ptr(), 1,
+                                            nat.stream_handle()), "plane")
+        return t
+
+    def set_plane(self, comp: int, plane: int, t):
+        t = t.to(self.dev, self.torch.float32).contiguous()
+        nat.check(self.lib.jxf_grid3d_plane(self.h, comp, plane, t.data_ptr(), 0,
+                                            nat.stream_handle()), "plane")
+
+    def half_step(self, half: int, probe_row=None):
+        nat.check(self.lib.jxf_grid3d_half_step(
+            self.h, half, None if probe_row is None else probe_row.data_ptr(),
+            nat.stream_handle()), "jxf_grid3d_half_step")
+
+    def new_probe_buffer(self, n_steps: int, n_local: int):
+        return self.torch.zeros((n_steps, n_local), dtype=self.torch.float32, device=self.dev)
+
+    def field(self, comp: int, local_shape):
+        t = self.torch.empty(local_shape, dtype=self.torch.float32, device=self.dev)
+        nat.check(self.lib.jxf_grid3d_get_field(self.h, comp, t.data_ptr(), 0,
+                                                nat.stream_handle()), "get_field")
+        return t
+
+    def check(self):
+        nat.check(self.lib.jxf_grid3d_check_error(self.h, nat.stream_handle()), "device error")
+
+
+class DistributedGrid3D:
+    """A 3D FDTD grid split along x over the ranks of a process group.
+
+    Every rank constructs it with the same arguments and makes the same calls
+    (collective semantics).  Sources, materials and probes use GLOBAL cell
+    indices.  ``run`` returns the full probe trace on every rank;
+    ``gather_field`` returns the full field on every rank.
+    """
+
+    def __init__(self, size, resolution=0.01, boundary="absorbing", pml_layers=8, *,
+                 cpml: CPMLSpec | None = None, group=None, device: int | None = None,
+                 stepper_factory=None):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.group = group
+        self.world = dist.get_world_size(group)
+        self.rank = dist.get_rank(group)
+        self.size = tuple(int(v) for v in size)
+        if min(self.size) < 8:
+            raise ConfigurationError(f"Grid must be at least 8x8x8, got {size}")
+        if boundary not in ("absorbing", "pec", "cpml"):
+            raise ConfigurationError(f"decomposed grids support absorbing, pec and cpml, not {boundary!r}")
+        self.dx = resolution
+        self.boundary = boundary
+        self.pml_layers = pml_layers
+        self.cpml = cpml or CPMLSpec()
+        self.ranges = slab_ranges(self.size[0], self.world)
+        self.x0, self.x1 = self.ranges[self.rank]
+        self.nloc = self.x1 - self.x0
+        self.dt = float(0.99 * resolution / (299792458.0 * float(np.sqrt(3.0))))
+        self.sources: list[PointSource3D] = []
+        self.probes: list[tuple[int, int, int, int]] = []
+        self.eps = None
+        if stepper_factory is None:
+            import torch
+
+            dev = device if device is not None else torch.cuda.current_device()
+
+            def stepper_factory(**kw):
+                return CudaSlabStepper(device=dev, **kw)
+
+        self.st = stepper_factory(size=self.size, x0=self.x0, x1=self.x1, dx=self.dx, dt=self.dt,
+                                  boundary=_BOUNDARY[boundary], pml_layers=pml_layers,
+                                  cpml=self.cpml)
+        self.local_shape = (self.nloc + 2, self.size[1], self.size[2])
+        self.step_count = 0
+        self._configured = False
+
+    # ----------------------------------------------------------- set-up
+    def add_source(self, s: PointSource3D):
+        ix, iy, iz = s.position
+        nx, ny, nz = self.size
+        if not (0 <= ix < nx and 0 <= iy < ny and 0 <= iz < nz):
+            raise ConfigurationError(f"Source position {s.position} out of grid bounds {self.size}")
+        self.sources.append(s)
+        self._configured = False
+
+    def add_probe(self, position, component="ez"):
+        ix, iy, iz = position
+        self.probes.append((int(ix), int(iy), int(iz), COMPONENTS.index(component)))
+        self._configured = False
+
+    def set_permittivity(self, eps_r):
+        arr = np.asarray(eps_r, dtype=np.float64)
+        if arr.shape != self.size:
+            raise ConfigurationError(f"permittivity shape {arr.shape} != grid size {self.size}")
+        self.eps = arr
+        self._configured = False
+
+    def _local_cell(self, ix, iy, iz):
+        ny, nz = self.size[1], self.size[2]
+        return ((ix - self.x0 + 1) * ny + iy) * nz + iz
+
+    def _configure(self, n_steps):
+        ny, nz = self.size[1], self.size[2]
+        if self.eps is not None:
+            lo, hi = self.x0 - 1, self.x1 + 1
+            loc = np.ones((self.nloc + 2, ny, nz))
+            a, b = max(lo, 0), min(hi, self.size[0])
+            loc[a - lo:b - lo] = self.eps[a:b]
+            self.st.set_eps(loc)
+        keys, cells, comps, amps, rows = [], [], [], [], []
+        for s in self.sources:
+            k = wf.waveform_key(s)
+            if k not in keys:
+                keys.append(k)
+            if self.x0 <= s.position[0] < self.x1:
+                cells.append(self._local_cell(*s.position))
+                comps.append(_POL[s.polarization])
+                amps.append(s.amplitude)
+                rows.append(keys.index(k))
+        self.st.set_sources(np.array(cells, np.int64), np.array(comps, np.int32),
+                            np.array(amps, np.float32), np.array(rows, np.int32))
+        self.st.set_waveforms(wf.build_table(keys, max(n_steps, 1), self.dt, 0.0))
+        self.own_probes = [i for i, p in enumerate(self.probes) if self.x0 <= p[0] < self.x1]
+        pc = np.array([self._local_cell(*self.probes[i][:3]) for i in self.own_probes], np.int64)
+        pk = np.array([self.probes[i][3] for i in self.own_probes], np.int32)
+        self.st.set_probes(pc, pk)
+        self.st.reset()
+        self.step_count = 0
+        self._configured = True
+
+    # ----------------------------------------------------------- exchange
+    def _exchange(self, comps, send_plane, recv_plane, direction):
+        """Swap one plane of `comps` with the neighbours: direction -1 sends
+        my plane to rank-1 and receives rank+1's into recv_plane; +1 the
+        other way.  gloo groups move the planes through host memory."""
+        import torch
+
+        r = self.rank
+        if direction < 0:
+            send_to = r - 1 if r > 0 else None
+            recv_from = r + 1 if r < self.world - 1 else None
+        else:
+            send_to = r + 1 if r < self.world - 1 else None
+            recv_from = r - 1 if r > 0 else None
+        on_host = self.dist.get_backend(self.group) == "gloo"
+        dev = torch.device("cpu") if on_host else self.st.device
+        dtype = self.st.dtype
+        ops, recv = [], None
+        if recv_from is not None:
+            recv = torch.empty((len(comps), self.size[1], self.size[2]), dtype=dtype, device=dev)
+            ops.append(self.dist.P2POp(self.dist.irecv, recv, recv_from, self.group))
+        if send_to is not None:
+            send = torch.stack([self.st.get_plane(c, send_plane) for c in comps]).to(dev, dtype)
+            ops.append(self.dist.P2POp(self.dist.isend, send.contiguous(), send_to, self.group))
+        if ops:
+            for req in self.dist.batch_isend_irecv(ops):
+                req.wait()
+        if recv is not None:
+            for k, c in enumerate(comps):
+                self.st.set_plane(c, recv_plane, recv[k])
+
+    # ----------------------------------------------------------- stepping
+    def run(self, n_steps: int):
+        """Advance from rest (first call) or from the current state; returns
+        the full probe trace (n_steps, n_probes) on every rank."""
+        import torch
+
+        if not self._configured:
+            self._configure(n_steps + self.step_count)
+            self._wave_len = n_steps + self.step_count
+        elif self.step_count + n_steps > self._wave_len:
+            # extend the waveform table (the state and step counter are kept)
+            keys = []
+            for s in self.sources:
+                k = wf.waveform_key(s)
+                if k not in keys:
+                    keys.append(k)
+            self._wave_len = 2 * (self.step_count + n_steps)
+            self.st.set_waveforms(wf.build_table(keys, self._wave_len, self.dt, 0.0))
+        buf = self.st.new_probe_buffer(n_steps, len(self.own_probes))
+        for k in range(n_steps):
+            # Ey, Ez of the next rank's first plane -> my high ghost plane
+            self._exchange((1, 2), 1, self.nloc + 1, -1)
+            self.st.half_step(0)
+            # Hy, Hz of the previous rank's last plane -> my low ghost plane
+            self._exchange((4, 5), self.nloc, 0, +1)
+            self.st.half_step(1, buf[k] if len(self.own_probes) else None)
+        self.step_count += n_steps
+        full = torch.zeros((n_steps, len(self.probes)), dtype=buf.dtype, device=buf.device)
+        if self.own_probes:
+            full[:, self.own_probes] = buf
+        if self.dist.get_backend(self.group) == "gloo":
+            host = full.cpu()
+            self.dist.all_reduce(host, group=self.group)
+            full = host.to(buf.device)
+        else:
+            self.dist.all_reduce(full, group=self.group)
+        return full
+
+    def gather_field(self, name: str):
+        """Full field (global shape) on every rank."""
+        import torch
+
+        c = COMPONENTS.index(name)
+        loc = self.st.field(c, self.local_shape)[1:self.nloc + 1].contiguous()
+        backend = self.dist.get_backend(self.group)
+        parts_shape = [(b - a, self.size[1], self.size[2]) for a, b in self.ranges]
+        src = loc.cpu() if backend == "gloo" else loc
+        # pad to the largest slab so all_gather sees equal shapes
+        m = max(s[0] for s in parts_shape)
+        pad = torch.zeros((m,) + self.size[1:], dtype=src.dtype, device=src.device)
+        pad[:loc.shape[0]] = src
+        outs = [torch.empty_like(pad) for _ in range(self.world)]
+        self.dist.all_gather(outs, pad, group=self.group)
+        full = torch.cat([o[:s[0]] for o, s in zip(outs, parts_shape)])
+        return full.to(loc.device)
+
+    def close(self):
+        self.st.close()
+
