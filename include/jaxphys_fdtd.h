@@ -167,6 +167,22 @@ int jxf_grid3d_half_step(jxf_grid3d* g, int32_t half, float* probe_row, void* st
 int jxf_grid3d_plane(jxf_grid3d* g, int32_t comp, int32_t plane, float* buf, int32_t to_buf,
                      void* stream);
 
+/* Batches of independent grids (extension; the reference runs one grid per
+ * simulate() call).  jxf_batch3d_create groups existing grids (generic path,
+ * same boundary mode and device; sizes may differ); they keep their own
+ * materials, sources, probes and field access.  jxf_batch3d_step advances
+ * every grid by n_steps with one kernel per phase for the whole batch; with
+ * use_graph != 0 the n-step sequence is captured once into a CUDA graph
+ * (cached per start step and length) and replayed with one launch.  Probe
+ * rows of the last run: jxf_batch3d_probes(b, grid, n_steps, dst) copies the
+ * [n_steps][n_probes of that grid] trace into device memory. */
+typedef struct jxf_batch3d jxf_batch3d;
+int jxf_batch3d_create(int32_t n, jxf_grid3d* const* grids, jxf_batch3d** out);
+int jxf_batch3d_destroy(jxf_batch3d* b);
+int jxf_batch3d_reset(jxf_batch3d* b, void* stream);
+int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_graph, void* stream);
+int jxf_batch3d_probes(jxf_batch3d* b, int32_t grid, int32_t n_steps, float* dst, void* stream);
+
 /* Zero fields and psi, reset the step counter. */
 int jxf_grid3d_reset(jxf_grid3d* g, void* stream);
 

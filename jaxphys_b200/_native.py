@@ -110,6 +110,11 @@ SIGNATURES = {
     "jxf_grid3d_create_slab": (C.c_int, [C.POINTER(Grid3DDesc), _i32, _i32, C.POINTER(_vp)]),
     "jxf_grid3d_half_step": (C.c_int, [_vp, _i32, _vp, _vp]),
     "jxf_grid3d_plane": (C.c_int, [_vp, _i32, _i32, _vp, _i32, _vp]),
+    "jxf_batch3d_create": (C.c_int, [_i32, C.POINTER(_vp), C.POINTER(_vp)]),
+    "jxf_batch3d_destroy": (C.c_int, [_vp]),
+    "jxf_batch3d_reset": (C.c_int, [_vp, _vp]),
+    "jxf_batch3d_step": (C.c_int, [_vp, _i32, _i32, _vp]),
+    "jxf_batch3d_probes": (C.c_int, [_vp, _i32, _i32, _vp, _vp]),
     "jxf_grid3d_run_noalloc": (C.c_int, [C.POINTER(NoAllocDesc), C.POINTER(_vp), _vp, _i32, _vp]),
     "jxf_grid2d_create": (C.c_int, [C.POINTER(Grid2DDesc), C.POINTER(_vp)]),
     "jxf_grid2d_destroy": (C.c_int, [_vp]),

@@ -1483,6 +1483,268 @@ int jxf_grid2d_check_error(jxf_grid2d* g, void* stream) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Batches of independent grids
+// ---------------------------------------------------------------------------
+
+struct jxf_batch3d {
+  std::vector<jxf_grid3d*> grids;
+  int mode = MODE_ABSORB;
+  int device = 0;
+  int64_t bytes = 0;
+  Step3D* d_params = nullptr;
+  int* d_blk_grid = nullptr;
+  int* d_blk_first = nullptr;
+  int* d_blk_count = nullptr;
+  int n_blocks = 0;
+  BatchSrcGrid* d_srcg = nullptr;
+  int2* d_src_entries = nullptr;
+  int n_src_entries = 0;
+  BatchProbe* d_probes = nullptr;
+  int n_probes = 0;
+  std::vector<int> probe_offset;  // first column of each grid in a probe row
+  float* d_probe_buf = nullptr;   // [n_steps][n_probes] of the last run
+  size_t probe_cap = 0;
+  long long step = 0;
+  cudaStream_t own = nullptr;     // capture stream when the caller passes the legacy stream
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_step0 = -1;
+  int graph_n = -1;
+  size_t cap[7] = {0, 0, 0, 0, 0, 0, 0};  // element capacity of the uploaded tables
+};
+
+namespace {
+
+int batch_refresh(jxf_batch3d* b) {
+  // parameters, block tables, sources and probes of every grid (cheap; done
+  // per call so later set_eps / set_sources on the member grids are seen)
+  std::vector<Step3D> params;
+  std::vector<int> bg, bf, bc;
+  std::vector<BatchSrcGrid> sg;
+  std::vector<int2> se;
+  std::vector<BatchProbe> pr;
+  b->probe_offset.clear();
+  int blocks = 0;
+  for (size_t k = 0; k < b->grids.size(); ++k) {
+    jxf_grid3d* g = b->grids[k];
+    Step3D p = base_params(g);
+    set_io(g, p, 0, 0);
+    params.push_back(p);
+    const long long cells = g->n;
+    const int nb = (int)std::max<long long>(1, std::min<long long>((cells + 255) / 256, 4096));
+    bf.push_back(blocks);
+    bc.push_back(nb);
+    for (int i = 0; i < nb; ++i) bg.push_back((int)k);
+    blocks += nb;
+    BatchSrcGrid s{};
+    for (int c = 0; c < 3; ++c) s.e[c] = g->f[0][c];
+    s.cells = g->d_cells;
+    s.terms = g->d_terms;
+    s.wave = g->d_wave;
+    s.wave_len = g->wave_len;
+    sg.push_back(s);
+    for (int i = 0; i < g->n_cells; ++i) se.push_back(make_int2((int)k, i));
+    b->probe_offset.push_back((int)pr.size());
+    if (g->n_probes > 0) {
+      std::vector<long long> cell(g->n_probes);
+      std::vector<int> comp(g->n_probes);
+      CUDA_TRY(cudaMemcpy(cell.data(), g->d_probe_cell, cell.size() * 8, cudaMemcpyDeviceToHost));
+      CUDA_TRY(cudaMemcpy(comp.data(), g->d_probe_comp, comp.size() * 4, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < g->n_probes; ++i) pr.push_back(BatchProbe{(int)k, comp[i], cell[i]});
+    }
+  }
+  if (b->n_blocks != blocks || b->n_src_entries != (int)se.size() ||
+      b->n_probes != (int)pr.size()) {
+    // launch shapes are part of a captured graph
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->n_blocks = blocks;
+  b->n_src_entries = (int)se.size();
+  b->n_probes = (int)pr.size();
+  // Copy into the existing buffers when they are large enough: a captured
+  // graph keeps these device addresses.  Any reallocation drops the graph.
+  bool moved = false;
+  auto put = [&](auto** ptr, size_t* cap, const auto& v) -> int {
+    if (v.empty()) return JXF_OK;
+    if (*cap < v.size()) {
+      dfree(*ptr);
+      TRY(dmalloc(ptr, v.size(), &b->bytes));
+      *cap = v.size();
+      moved = true;
+    }
+    CUDA_TRY(cudaMemcpy(*ptr, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice));
+    return JXF_OK;
+  };
+  TRY(put(&b->d_params, &b->cap[0], params));
+  TRY(put(&b->d_blk_grid, &b->cap[1], bg));
+  TRY(put(&b->d_blk_first, &b->cap[2], bf));
+  TRY(put(&b->d_blk_count, &b->cap[3], bc));
+  TRY(put(&b->d_srcg, &b->cap[4], sg));
+  TRY(put(&b->d_src_entries, &b->cap[5], se));
+  TRY(put(&b->d_probes, &b->cap[6], pr));
+  if (moved && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return JXF_OK;
+}
+
+// One leapfrog step of every grid (kernels only; capturable).
+int batch_launch_step(jxf_batch3d* b, long long step, float* probe_row, cudaStream_t st) {
+  BatchBlocks bb{b->d_params, b->d_blk_grid, b->d_blk_first, b->d_blk_count};
+  if (b->mode == MODE_CPML) {
+    k3d_batch_h<MODE_CPML><<<b->n_blocks, 256, 0, st>>>(bb);
+    k3d_batch_e<MODE_CPML><<<b->n_blocks, 256, 0, st>>>(bb);
+  } else {
+    k3d_batch_h<MODE_ABSORB><<<b->n_blocks, 256, 0, st>>>(bb);
+    k3d_batch_e<MODE_ABSORB><<<b->n_blocks, 256, 0, st>>>(bb);
+  }
+  if (b->n_src_entries > 0)
+    k3d_batch_sources<<<(b->n_src_entries + 127) / 128, 128, 0, st>>>(b->d_srcg, b->d_src_entries,
+                                                                      b->n_src_entries, step);
+  if (probe_row && b->n_probes > 0)
+    k3d_batch_probes<<<(b->n_probes + 127) / 128, 128, 0, st>>>(b->d_params, b->d_probes,
+                                                                b->n_probes, probe_row);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+}  // namespace
+
+extern "C" int jxf_batch3d_create(int32_t n, jxf_grid3d* const* grids, jxf_batch3d** out) {
+  if (!out || n < 1 || !grids) return fail(JXF_ERR_INVALID, "need at least one grid");
+  *out = nullptr;
+  const int mode = grids[0]->mode;
+  const int dev = grids[0]->d.device;
+  for (int i = 0; i < n; ++i) {
+    const jxf_grid3d* g = grids[i];
+    if (!g) return fail(JXF_ERR_INVALID, "grid %d is null", i);
+    if (g->path != JXF_PATH_GENERIC || g->slab)
+      return fail(JXF_ERR_INVALID, "grid %d: batched grids use the generic path", i);
+    if (g->mode != mode || g->d.device != dev)
+      return fail(JXF_ERR_INVALID, "grid %d: batched grids share the boundary mode and device", i);
+    if (g->mode == MODE_PERIODIC) return fail(JXF_ERR_INVALID, "periodic grids are not batched");
+  }
+  DeviceGuard dg(dev);
+  jxf_batch3d* b = new jxf_batch3d();
+  b->grids.assign(grids, grids + n);
+  b->mode = mode;
+  b->device = dev;
+  int rc = batch_refresh(b);
+  if (rc != JXF_OK) {
+    jxf_batch3d_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return JXF_OK;
+}
+
+extern "C" int jxf_batch3d_destroy(jxf_batch3d* b) {
+  if (!b) return JXF_OK;
+  DeviceGuard dg(b->device);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->own) cudaStreamDestroy(b->own);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  dfree(b->d_params);
+  dfree(b->d_blk_grid);
+  dfree(b->d_blk_first);
+  dfree(b->d_blk_count);
+  dfree(b->d_srcg);
+  dfree(b->d_src_entries);
+  dfree(b->d_probes);
+  dfree(b->d_probe_buf);
+  delete b;
+  return JXF_OK;
+}
+
+extern "C" int jxf_batch3d_reset(jxf_batch3d* b, void* stream) {
+  if (!b) return fail(JXF_ERR_INVALID, "null handle");
+  for (jxf_grid3d* g : b->grids) TRY(jxf_grid3d_reset(g, stream));
+  b->step = 0;
+  return JXF_OK;
+}
+
+extern "C" int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_graph, void* stream) {
+  if (!b) return fail(JXF_ERR_INVALID, "null handle");
+  if (n_steps < 0) return fail(JXF_ERR_INVALID, "n_steps must be >= 0");
+  if (n_steps == 0) return JXF_OK;
+  for (jxf_grid3d* g : b->grids) {
+    if (!g->src_cell.empty() && b->step + n_steps > g->wave_len)
+      return fail(JXF_ERR_INVALID, "a member grid's waveform table is too short");
+  }
+  DeviceGuard dg(b->device);
+  TRY(batch_refresh(b));
+  const size_t need = (size_t)n_steps * std::max(b->n_probes, 1);
+  if (need > b->probe_cap) {
+    dfree(b->d_probe_buf);
+    TRY(dmalloc(&b->d_probe_buf, need, &b->bytes));
+    b->probe_cap = need;
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!use_graph) {
+    for (int k = 0; k < n_steps; ++k)
+      TRY(batch_launch_step(b, b->step + k,
+                            b->n_probes ? b->d_probe_buf + (size_t)k * b->n_probes : nullptr, st));
+  } else {
+    if (!b->own) {
+      CUDA_TRY(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
+      CUDA_TRY(cudaEventCreateWithFlags(&b->ev0, cudaEventDisableTiming));
+      CUDA_TRY(cudaEventCreateWithFlags(&b->ev1, cudaEventDisableTiming));
+    }
+    if (!b->graph || b->graph_n != n_steps || b->graph_step0 != b->step) {
+      if (b->graph) cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+      cudaGraph_t graph;
+      CUDA_TRY(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < n_steps; ++k) {
+        int rc = batch_launch_step(
+            b, b->step + k, b->n_probes ? b->d_probe_buf + (size_t)k * b->n_probes : nullptr,
+            b->own);
+        if (rc != JXF_OK) {
+          cudaStreamEndCapture(b->own, &graph);
+          return rc;
+        }
+      }
+      CUDA_TRY(cudaStreamEndCapture(b->own, &graph));
+      CUDA_TRY(cudaGraphInstantiate(&b->graph, graph, 0));
+      cudaGraphDestroy(graph);
+      b->graph_n = n_steps;
+      b->graph_step0 = b->step;
+    }
+    // order the graph between the caller's earlier and later work
+    CUDA_TRY(cudaEventRecord(b->ev0, st));
+    CUDA_TRY(cudaStreamWaitEvent(b->own, b->ev0, 0));
+    CUDA_TRY(cudaGraphLaunch(b->graph, b->own));
+    CUDA_TRY(cudaEventRecord(b->ev1, b->own));
+    CUDA_TRY(cudaStreamWaitEvent(st, b->ev1, 0));
+  }
+  b->step += n_steps;
+  for (jxf_grid3d* g : b->grids) g->step += n_steps;
+  return JXF_OK;
+}
+
+extern "C" int jxf_batch3d_probes(jxf_batch3d* b, int32_t grid, int32_t n_steps, float* dst,
+                                  void* stream) {
+  if (!b || !dst) return fail(JXF_ERR_INVALID, "null argument");
+  if (grid < 0 || grid >= (int)b->grids.size()) return fail(JXF_ERR_INVALID, "grid out of range");
+  const int np = b->grids[grid]->n_probes;
+  if (np == 0) return JXF_OK;
+  if ((size_t)n_steps * b->n_probes > b->probe_cap)
+    return fail(JXF_ERR_INVALID, "no probe rows for %d steps", n_steps);
+  DeviceGuard dg(b->device);
+  CUDA_TRY(cudaMemcpy2DAsync(dst, np * 4, b->d_probe_buf + b->probe_offset[grid],
+                             (size_t)b->n_probes * 4, np * 4, n_steps, cudaMemcpyDeviceToDevice,
+                             (cudaStream_t)stream));
+  return JXF_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Adjoint (permittivity gradients of probe objectives)
 // ---------------------------------------------------------------------------
 

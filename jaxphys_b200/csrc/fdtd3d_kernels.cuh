@@ -151,8 +151,9 @@ __device__ __forceinline__ PsiTerm g_term(const CpmlDev& P, int id, bool on, flo
   return PsiTerm{on, b, c, ik, on ? P.out[id][idx] : 0.0f, on ? P.out[id] + idx : nullptr};
 }
 
+// Body of the generic H pass over the owned cells k0, k0+kstep, ...
 template <int MODE>
-__global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Step3D p) {
+__device__ __forceinline__ void generic_h_body(const Step3D& p, long long k0, long long kstep) {
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const long long plane = (long long)ny * nz;
   const long long n = (long long)(p.x_hi - p.x_lo) * plane;  // owned cells
@@ -161,8 +162,7 @@ __global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Ste
   const float* ex = p.in[0];
   const float* ey = p.in[1];
   const float* ez = p.in[2];
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
+  for (long long k = k0; k < n; k += kstep) {
     const long long idx = base + k;
     const int z = (int)(idx % nz);
     const long long t = idx / nz;
@@ -228,8 +228,9 @@ __global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Ste
   }
 }
 
+// Body of the generic E pass over the owned cells k0, k0+kstep, ...
 template <int MODE>
-__global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Step3D p) {
+__device__ __forceinline__ void generic_e_body(const Step3D& p, long long k0, long long kstep) {
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const long long plane = (long long)ny * nz;
   const long long n = (long long)(p.x_hi - p.x_lo) * plane;  // owned cells
@@ -237,8 +238,7 @@ __global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Ste
   const float* hx = p.out[3];  // H already advanced (in place)
   const float* hy = p.out[4];
   const float* hz = p.out[5];
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
+  for (long long k = k0; k < n; k += kstep) {
     const long long idx = base + k;
     const int z = (int)(idx % nz);
     const long long t = idx / nz;
@@ -309,6 +309,41 @@ __global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Ste
   }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(256) k3d_generic_h(const __grid_constant__ Step3D p) {
+  generic_h_body<MODE>(p, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+                       (long long)gridDim.x * blockDim.x);
+}
+template <int MODE>
+__global__ void __launch_bounds__(256) k3d_generic_e(const __grid_constant__ Step3D p) {
+  generic_e_body<MODE>(p, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+                       (long long)gridDim.x * blockDim.x);
+}
+
+// Batched passes: many independent grids in one launch.  Block b works on
+// grid blk_grid[b] (its blk_count[g] blocks start at blk_first[g]); each grid's
+// parameters are read from global memory.
+struct BatchBlocks {
+  const Step3D* grids;
+  const int* blk_grid;
+  const int* blk_first;
+  const int* blk_count;
+};
+template <int MODE>
+__global__ void __launch_bounds__(256) k3d_batch_h(const __grid_constant__ BatchBlocks b) {
+  const int g = b.blk_grid[blockIdx.x];
+  generic_h_body<MODE>(b.grids[g],
+                       (long long)(blockIdx.x - b.blk_first[g]) * blockDim.x + threadIdx.x,
+                       (long long)b.blk_count[g] * blockDim.x);
+}
+template <int MODE>
+__global__ void __launch_bounds__(256) k3d_batch_e(const __grid_constant__ BatchBlocks b) {
+  const int g = b.blk_grid[blockIdx.x];
+  generic_e_body<MODE>(b.grids[g],
+                       (long long)(blockIdx.x - b.blk_first[g]) * blockDim.x + threadIdx.x,
+                       (long long)b.blk_count[g] * blockDim.x);
+}
+
 // Soft sources, grouped by cell (list order within a cell), after the E update.
 __global__ void k3d_sources(float* ex, float* ey, float* ez, const SrcCell* cells, int n_cells,
                             const SrcTerm* terms, const float* wave, long long wave_len,
@@ -323,6 +358,42 @@ __global__ void k3d_sources(float* ex, float* ey, float* ez, const SrcCell* cell
     v = fadd(v, fmul(t.amp, wave[(long long)t.wave * wave_len + step]));
   }
   f[c.cell] = v;
+}
+
+// Batched soft sources: one thread per (grid, source cell) entry.
+struct BatchSrcGrid {
+  float* e[3];
+  const SrcCell* cells;
+  const SrcTerm* terms;
+  const float* wave;
+  long long wave_len;
+};
+__global__ void k3d_batch_sources(const BatchSrcGrid* grids, const int2* entries, int n,
+                                  long long step) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int2 en = entries[i];
+  const BatchSrcGrid& g = grids[en.x];
+  const SrcCell c = g.cells[en.y];
+  float* f = g.e[c.comp];
+  float v = f[c.cell];
+  for (int k = 0; k < c.count; ++k) {
+    const SrcTerm t = g.terms[c.first + k];
+    v = fadd(v, fmul(t.amp, g.wave[(long long)t.wave * g.wave_len + step]));
+  }
+  f[c.cell] = v;
+}
+
+// Batched probes: out[i] = grids[g_i].in[comp_i][cell_i] (state after the step)
+struct BatchProbe {
+  int grid, comp;
+  long long cell;
+};
+__global__ void k3d_batch_probes(const Step3D* grids, const BatchProbe* pr, int n, float* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const BatchProbe q = pr[i];
+  out[i] = grids[q.grid].in[q.comp][q.cell];
 }
 
 struct FieldPtrs6 {

@@ -1,0 +1,79 @@
+"""Batches of independent 3D grids advanced together (extension).
+
+``FDTDBatch(grids)`` takes ``EMGrid3D`` objects (generic kernel path; any
+mix of sizes, including odd ones; one boundary mode) and advances all of them
+with one kernel per phase per step over the whole batch (C ABI
+``jxf_batch3d_*``).  ``run(n)`` captures the n-step sequence once into a CUDA
+graph and replays it with a single launch.  Each grid keeps its own
+permittivity, sources, probes and field accessors.  Typical use: many design
+candidates, or many source positions, of one device.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+from .. import _native as nat
+from ..exceptions import ConfigurationError
+
+
+class FDTDBatch:
+    def __init__(self, grids):
+        if not grids:
+            raise ConfigurationError("empty batch")
+        for g in grids:
+            if g._path != "generic":
+                raise ConfigurationError("batched grids must be built with path='generic'")
+            if g._h is None:
+                g.prepare(g._dt, g._t_start)
+            elif g._dirty:
+                g._upload_config()
+        self.grids = list(grids)
+        lib = nat.load()
+        arr = (C.c_void_p * len(grids))(*[g._h for g in grids])
+        h = C.c_void_p()
+        nat.check(lib.jxf_batch3d_create(len(grids), arr, C.byref(h)), "jxf_batch3d_create")
+        self._h = h
+        self._last_n = 0
+
+    def close(self):
+        if self._h is not None:
+            nat.load().jxf_batch3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self):
+        nat.check(nat.load().jxf_batch3d_reset(self._h, nat.stream_handle()), "batch reset")
+
+    @property
+    def cells(self) -> int:
+        return sum(g.size[0] * g.size[1] * g.size[2] for g in self.grids)
+
+    def run(self, n_steps: int, use_graph: bool = True):
+        """Advance every grid by n_steps; returns the probe traces of each grid
+        (device tensors (n_steps, P_g), None for grids without probes)."""
+        import torch
+
+        for g in self.grids:
+            if g._dirty:
+                g._upload_config()
+            if g._sources:
+                g._ensure_waves(g.step_count + int(n_steps))
+        nat.check(nat.load().jxf_batch3d_step(self._h, int(n_steps), 1 if use_graph else 0,
+                                              nat.stream_handle()), "jxf_batch3d_step")
+        out = []
+        for i, g in enumerate(self.grids):
+            if not g._probes:
+                out.append(None)
+                continue
+            t = torch.empty((int(n_steps), len(g._probes)), dtype=torch.float32,
+                            device=f"cuda:{g._h_key[1]}")
+            nat.check(nat.load().jxf_batch3d_probes(self._h, i, int(n_steps), t.data_ptr(),
+                                                    nat.stream_handle()), "batch probes")
+            out.append(t)
+        return out

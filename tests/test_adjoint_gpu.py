@@ -65,7 +65,7 @@ def test_adjoint_matches_fp64_autodiff(cuda, bnd):
                      probes=probes)
     J64, grad64, tr64 = torch_ref.grad_eps(spec, eps, n, dt, w)
     assert rel_l2(to_np(tr), tr64) <= 1e-5
-    assert abs(float(J) - J64) <= 1e-5 * abs(J64)
+    assert abs(J.item() - J64) <= 1e-5 * abs(J64)
     e_rel = rel_l2(grad, grad64)
     assert e_rel <= 1e-3, e_rel
     # the forward of the adjoint run is the regular forward
