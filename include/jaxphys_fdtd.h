@@ -183,6 +183,51 @@ int jxf_batch3d_reset(jxf_batch3d* b, void* stream);
 int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_graph, void* stream);
 int jxf_batch3d_probes(jxf_batch3d* b, int32_t grid, int32_t n_steps, float* dst, void* stream);
 
+/* Learned absorbing band (extension; the reference has only the graded PML).
+ * A jxf_band holds one small network per face of a box (6 faces,
+ * f = 2 * axis + side): 54 inputs (the 3 x 3 stencil of Ex..Hz, H scaled by
+ * eta0, over the 3 outermost cell layers along the face normal and
+ * -1, 0, +1 along its first tangent axis, normalised by their RMS s),
+ * 2 hidden layers of 64 (tanh-form GELU), 6 outputs; BF16 weights, FP32
+ * accumulation on the tensor cores.  After each plain step of a PEC-walled
+ * grid, every cell of the outer layer gets X += s * output (H / eta0).
+ * Parameters per face (FP32, JXF_BAND_PARAMS floats): W1[64][64] (out, in;
+ * inputs 54..63 zero), b1[64], W2[64][64], b2[64], W3[16][64] (rows 6..15
+ * zero), b3[16].
+ *   jxf_band_collect   appends training rows for the outer cells of a grid
+ *                      given by 6 device field pointers (its state after one
+ *                      plain step from a reference state) against the
+ *                      reference's next state (6 device pointers of a larger
+ *                      grid, the box at offset (ox, oy, oz)); row weight s^2.
+ *   jxf_band_grad      gradient and loss (sum of w |out - target|^2 / sum w,
+ *                      per face) over the whole dataset, no update.
+ *   jxf_band_train     iters Adam steps on batch_rows random rows per face;
+ *                      loss[i] (nullable) = summed face losses of step i.
+ *   jxf_band_eval      outputs for given normalised feature rows (testing).
+ *   jxf_batch3d_set_band attaches a band to a batch of PEC grids (NULL
+ *                      detaches); every later step applies it. */
+#define JXF_BAND_PARAMS 9360
+#define JXF_BAND_FACES 6
+#define JXF_BAND_FEATURES 54
+typedef struct jxf_band jxf_band;
+int jxf_band_create(int32_t device, jxf_band** out);
+int jxf_band_destroy(jxf_band* m);
+int jxf_band_set_params(jxf_band* m, const float* params);
+int jxf_band_get_params(jxf_band* m, float* params);
+int jxf_band_eval(jxf_band* m, int32_t n, const float* feat, const int32_t* face, float* out);
+int jxf_band_collect(jxf_band* m, float* const* fields, int32_t nx, int32_t ny, int32_t nz,
+                     const float* const* ref, int32_t rnx, int32_t rny, int32_t rnz, int32_t ox,
+                     int32_t oy, int32_t oz, void* stream);
+int jxf_band_dataset_size(jxf_band* m, int64_t* rows);
+int jxf_band_dataset_clear(jxf_band* m);
+int jxf_band_dataset_get(jxf_band* m, int32_t face, int64_t first, int64_t count, uint16_t* feat,
+                         float* target, float* weight);
+int jxf_band_grad(jxf_band* m, float* grad, float* loss, void* stream);
+int jxf_band_train(jxf_band* m, int32_t iters, int32_t batch_rows, float lr, uint64_t seed,
+                   float* loss, void* stream);
+int jxf_band_check_error(jxf_band* m, void* stream);
+int jxf_batch3d_set_band(jxf_batch3d* b, jxf_band* m);
+
 /* Zero fields and psi, reset the step counter. */
 int jxf_grid3d_reset(jxf_grid3d* g, void* stream);
 

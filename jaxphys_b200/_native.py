@@ -75,6 +75,11 @@ class Grid2DDesc(C.Structure):
     ]
 
 
+# learned band layout (include/jaxphys_fdtd.h)
+BAND_PARAMS = 9360
+BAND_FACES = 6
+BAND_FEATURES = 54
+
 _vp = C.c_void_p
 _i32 = C.c_int32
 _i64 = C.c_int64
@@ -115,6 +120,20 @@ SIGNATURES = {
     "jxf_batch3d_reset": (C.c_int, [_vp, _vp]),
     "jxf_batch3d_step": (C.c_int, [_vp, _i32, _i32, _vp]),
     "jxf_batch3d_probes": (C.c_int, [_vp, _i32, _i32, _vp, _vp]),
+    "jxf_band_create": (C.c_int, [_i32, C.POINTER(_vp)]),
+    "jxf_band_destroy": (C.c_int, [_vp]),
+    "jxf_band_set_params": (C.c_int, [_vp, _vp]),
+    "jxf_band_get_params": (C.c_int, [_vp, _vp]),
+    "jxf_band_eval": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),
+    "jxf_band_collect": (C.c_int, [_vp, C.POINTER(_vp), _i32, _i32, _i32, C.POINTER(_vp), _i32,
+                                   _i32, _i32, _i32, _i32, _i32, _vp]),
+    "jxf_band_dataset_size": (C.c_int, [_vp, _vp]),
+    "jxf_band_dataset_clear": (C.c_int, [_vp]),
+    "jxf_band_dataset_get": (C.c_int, [_vp, _i32, _i64, _i64, _vp, _vp, _vp]),
+    "jxf_band_grad": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "jxf_band_train": (C.c_int, [_vp, _i32, _i32, C.c_float, C.c_uint64, _vp, _vp]),
+    "jxf_band_check_error": (C.c_int, [_vp, _vp]),
+    "jxf_batch3d_set_band": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_run_noalloc": (C.c_int, [C.POINTER(NoAllocDesc), C.POINTER(_vp), _vp, _i32, _vp]),
     "jxf_grid2d_create": (C.c_int, [C.POINTER(Grid2DDesc), C.POINTER(_vp)]),
     "jxf_grid2d_destroy": (C.c_int, [_vp]),

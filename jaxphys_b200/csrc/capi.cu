@@ -21,6 +21,7 @@
 #include "fdtd2d_kernels.cuh"
 #include "fdtd3d_adjoint.cuh"
 #include "fdtd3d_kernels.cuh"
+#include "learned_band.cuh"
 
 using namespace jxf;
 
@@ -1511,7 +1512,20 @@ struct jxf_batch3d {
   long long graph_step0 = -1;
   int graph_n = -1;
   size_t cap[7] = {0, 0, 0, 0, 0, 0, 0};  // element capacity of the uploaded tables
+  // learned absorbing band (PEC batches only)
+  jxf_band* band = nullptr;
+  band::GridRef* d_band_grids = nullptr;
+  int2* d_band_cells = nullptr;
+  int* d_band_tile_face = nullptr;
+  float* d_band_delta = nullptr;
+  int band_tiles = 0;
+  int band_ctas = 0;
 };
+
+namespace {
+int band_launch(jxf_band* m, const band::GridRef* grids, const int2* cells, const int* tile_face,
+                int n_tiles, int ctas, float* delta, cudaStream_t st);
+}
 
 namespace {
 
@@ -1603,6 +1617,9 @@ int batch_launch_step(jxf_batch3d* b, long long step, float* probe_row, cudaStre
   if (b->n_src_entries > 0)
     k3d_batch_sources<<<(b->n_src_entries + 127) / 128, 128, 0, st>>>(b->d_srcg, b->d_src_entries,
                                                                       b->n_src_entries, step);
+  if (b->band && b->band_tiles > 0)
+    TRY(band_launch(b->band, b->d_band_grids, b->d_band_cells, b->d_band_tile_face,
+                    b->band_tiles, b->band_ctas, b->d_band_delta, st));
   if (probe_row && b->n_probes > 0)
     k3d_batch_probes<<<(b->n_probes + 127) / 128, 128, 0, st>>>(b->d_params, b->d_probes,
                                                                 b->n_probes, probe_row);
@@ -1655,6 +1672,10 @@ extern "C" int jxf_batch3d_destroy(jxf_batch3d* b) {
   dfree(b->d_src_entries);
   dfree(b->d_probes);
   dfree(b->d_probe_buf);
+  dfree(b->d_band_grids);
+  dfree(b->d_band_cells);
+  dfree(b->d_band_tile_face);
+  dfree(b->d_band_delta);
   delete b;
   return JXF_OK;
 }
@@ -1743,6 +1764,587 @@ extern "C" int jxf_batch3d_probes(jxf_batch3d* b, int32_t grid, int32_t n_steps,
                              (cudaStream_t)stream));
   return JXF_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Learned absorbing band
+// ---------------------------------------------------------------------------
+
+struct jxf_band {
+  int device = 0;
+  int64_t bytes = 0;
+  float* d_params = nullptr;  // [6][kParams] FP32 master
+  float* d_grad = nullptr;
+  float* d_m1 = nullptr;
+  float* d_m2 = nullptr;
+  unsigned char* d_wimg = nullptr;  // [6][kImgBytes] BF16 operand images
+  float* d_loss = nullptr;          // [loss_cap][6]
+  size_t loss_cap = 0;
+  double* d_wsum = nullptr;         // [6] sum of row weights
+  int* d_err = nullptr;
+  long long adam_t = 0;
+  // training rows per face
+  __nv_bfloat16* feat[6] = {};
+  float* tgt[6] = {};
+  float* w[6] = {};
+  long long rows[6] = {};
+  long long cap[6] = {};
+  int* d_cells = nullptr;  // collect scratch
+  size_t cells_cap = 0;
+};
+
+namespace {
+
+int band_setup_attrs() {
+  static int done = 0;
+  if (!done) {
+    CUDA_TRY(cudaFuncSetAttribute(band::k_band_infer<band::SRC_GRIDS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, band::kInfSmem));
+    CUDA_TRY(cudaFuncSetAttribute(band::k_band_infer<band::SRC_ROWS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, band::kInfSmem));
+    CUDA_TRY(cudaFuncSetAttribute(band::k_band_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  band::kTrSmem));
+    done = 1;
+  }
+  return JXF_OK;
+}
+
+// Owning face of an outer-layer cell, or -1 for an inner cell.
+int band_owner(int x, int y, int z, int nx, int ny, int nz) {
+  const int c[3] = {x, y, z}, n[3] = {nx, ny, nz};
+  int ax[3], sd[3], k = 0;
+  for (int a = 0; a < 3; ++a) {
+    if (c[a] == 0) {
+      ax[k] = a;
+      sd[k++] = 0;
+    } else if (c[a] == n[a] - 1) {
+      ax[k] = a;
+      sd[k++] = 1;
+    }
+  }
+  if (k == 0) return -1;
+  if (k == 1 || k == 3) return 2 * ax[0] + sd[0];
+  const int a = ax[0], b = ax[1];
+  return (b == (a + 1) % 3) ? 2 * a + sd[0] : 2 * b + sd[1];
+}
+
+// Outer-layer cells of an nx*ny*nz grid, per owning face, ascending.
+void band_cells(int nx, int ny, int nz, std::vector<int> out[6]) {
+  for (int f = 0; f < 6; ++f) out[f].clear();
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y) {
+      const bool full = x == 0 || x == nx - 1 || y == 0 || y == ny - 1;
+      for (int z = 0; z < nz; z += (full || z == nz - 1) ? 1 : nz - 1) {
+        const int f = band_owner(x, y, z, nx, ny, nz);
+        if (f >= 0) out[f].push_back((x * ny + y) * nz + z);
+      }
+    }
+}
+
+int band_check_dims(int nx, int ny, int nz) {
+  if (nx < 8 || ny < 8 || nz < 8)
+    return fail(JXF_ERR_INVALID, "a learned band needs every grid side >= 8 (got %d x %d x %d)",
+                nx, ny, nz);
+  if ((long long)nx * ny * nz >= (1ll << 31))
+    return fail(JXF_ERR_INVALID, "a learned band grid must have fewer than 2^31 cells");
+  return JXF_OK;
+}
+
+int band_launch(jxf_band* m, const band::GridRef* grids, const int2* cells, const int* tile_face,
+                int n_tiles, int ctas, float* delta, cudaStream_t st) {
+  band::InferArgs a{};
+  a.grids = grids;
+  a.cells = cells;
+  a.tile_face = tile_face;
+  a.n_tiles = n_tiles;
+  a.wimg = m->d_wimg;
+  a.params = m->d_params;
+  a.delta = delta;
+  a.err = m->d_err;
+  a.wait_ns = wait_limit_ns();
+  band::k_band_infer<band::SRC_GRIDS><<<ctas, 128, band::kInfSmem, st>>>(a);
+  const int n = n_tiles * band::kTile;
+  band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(grids, cells, n, delta);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+// CTAs of the inference kernel: resident CTAs per SM (at most 4, which also
+// keeps 4 x 128 TMEM columns within the SM's 512) times the SM count.
+int band_ctas(int n_tiles, int device) {
+  int sms = 148, occ = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, band::k_band_infer<band::SRC_GRIDS>, 128,
+                                                band::kInfSmem);
+  occ = std::max(1, std::min(occ, 4));
+  return std::max(1, std::min(n_tiles, sms * occ));
+}
+
+// Face lists -> padded tile arrays.
+void band_tiles(const std::vector<int2> per_face[6], std::vector<int2>& cells,
+                std::vector<int>& tile_face) {
+  cells.clear();
+  tile_face.clear();
+  for (int f = 0; f < 6; ++f) {
+    const size_t n = per_face[f].size();
+    const size_t nt = (n + band::kTile - 1) / band::kTile;
+    for (size_t t = 0; t < nt; ++t) tile_face.push_back(f);
+    for (size_t i = 0; i < nt * band::kTile; ++i)
+      cells.push_back(i < n ? per_face[f][i] : make_int2(-1, 0));
+  }
+}
+
+int band_grow(jxf_band* m, int f, long long need) {
+  if (need <= m->cap[f]) return JXF_OK;
+  long long nc = std::max<long long>(need, std::max<long long>(65536, m->cap[f] * 2));
+  __nv_bfloat16* nf = nullptr;
+  float *nt = nullptr, *nw = nullptr;
+  TRY(dmalloc(&nf, (size_t)nc * band::kInP, &m->bytes));
+  TRY(dmalloc(&nt, (size_t)nc * band::kOut, &m->bytes));
+  TRY(dmalloc(&nw, (size_t)nc, &m->bytes));
+  if (m->rows[f] > 0) {
+    CUDA_TRY(cudaMemcpy(nf, m->feat[f], (size_t)m->rows[f] * band::kInP * 2,
+                        cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(nt, m->tgt[f], (size_t)m->rows[f] * band::kOut * 4,
+                        cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(nw, m->w[f], (size_t)m->rows[f] * 4, cudaMemcpyDeviceToDevice));
+  }
+  m->bytes -= (int64_t)m->cap[f] * (band::kInP * 2 + band::kOut * 4 + 4);
+  dfree(m->feat[f]);
+  dfree(m->tgt[f]);
+  dfree(m->w[f]);
+  m->feat[f] = nf;
+  m->tgt[f] = nt;
+  m->w[f] = nw;
+  m->cap[f] = nc;
+  return JXF_OK;
+}
+
+__global__ void k_band_wsum(const float* w, long long n, double* out) {
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    s += w[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+int band_weight_sums(jxf_band* m, double out[6], cudaStream_t st) {
+  CUDA_TRY(cudaMemsetAsync(m->d_wsum, 0, 6 * sizeof(double), st));
+  for (int f = 0; f < 6; ++f)
+    if (m->rows[f] > 0)
+      k_band_wsum<<<256, 256, 0, st>>>(m->w[f], m->rows[f], m->d_wsum + f);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(out, m->d_wsum, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return JXF_OK;
+}
+
+int band_pack(jxf_band* m, cudaStream_t st) {
+  band::k_band_pack<<<dim3((band::kImgBytes / 2 + 255) / 256, 6), 256, 0, st>>>(m->d_params,
+                                                                                m->d_wimg);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+int band_train_pass(jxf_band* m, const band::TrainArgs& a, cudaStream_t st) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+  int maxt = 0;
+  for (int f = 0; f < 6; ++f) maxt = std::max(maxt, a.tiles[f]);
+  if (maxt == 0) return JXF_OK;
+  const int gx = std::max(1, std::min(maxt, std::max(1, sms / 6)));
+  band::k_band_train<<<dim3(gx, 6), 128, band::kTrSmem, st>>>(a);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+band::TrainArgs band_train_args(jxf_band* m) {
+  band::TrainArgs a{};
+  for (int f = 0; f < 6; ++f) {
+    a.feat[f] = m->feat[f];
+    a.tgt[f] = m->tgt[f];
+    a.w[f] = m->w[f];
+    a.count[f] = m->rows[f];
+  }
+  a.wimg = m->d_wimg;
+  a.params = m->d_params;
+  a.grad = m->d_grad;
+  a.err = m->d_err;
+  a.wait_ns = wait_limit_ns();
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jxf_band_create(int32_t device, jxf_band** out) {
+  if (!out) return fail(JXF_ERR_INVALID, "null output");
+  *out = nullptr;
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(JXF_ERR_INVALID, "device %d out of range", device);
+  DeviceGuard dg(device);
+  TRY(band_setup_attrs());
+  jxf_band* m = new jxf_band();
+  m->device = device;
+  const size_t np = 6 * (size_t)band::kParams;
+  int rc = JXF_OK;
+  if (rc == JXF_OK) rc = dmalloc(&m->d_params, np, &m->bytes);
+  if (rc == JXF_OK) rc = dmalloc(&m->d_grad, np, &m->bytes);
+  if (rc == JXF_OK) rc = dmalloc(&m->d_m1, np, &m->bytes);
+  if (rc == JXF_OK) rc = dmalloc(&m->d_m2, np, &m->bytes);
+  if (rc == JXF_OK) rc = dmalloc(&m->d_wimg, 6 * (size_t)band::kImgBytes, &m->bytes);
+  if (rc == JXF_OK) rc = dmalloc(&m->d_wsum, 6, &m->bytes);
+  if (rc == JXF_OK) rc = dmalloc(&m->d_err, 4, &m->bytes);
+  if (rc == JXF_OK && cudaMemset(m->d_params, 0, np * 4) != cudaSuccess) rc = JXF_ERR_CUDA;
+  if (rc == JXF_OK && cudaMemset(m->d_m1, 0, np * 4) != cudaSuccess) rc = JXF_ERR_CUDA;
+  if (rc == JXF_OK && cudaMemset(m->d_m2, 0, np * 4) != cudaSuccess) rc = JXF_ERR_CUDA;
+  if (rc == JXF_OK && cudaMemset(m->d_err, 0, 16) != cudaSuccess) rc = JXF_ERR_CUDA;
+  if (rc == JXF_OK) rc = band_pack(m, 0);
+  if (rc == JXF_OK && cudaDeviceSynchronize() != cudaSuccess) rc = JXF_ERR_CUDA;
+  if (rc != JXF_OK) {
+    jxf_band_destroy(m);
+    return rc == JXF_ERR_CUDA ? fail(rc, "band allocation failed") : rc;
+  }
+  *out = m;
+  return JXF_OK;
+}
+
+int jxf_band_destroy(jxf_band* m) {
+  if (!m) return JXF_OK;
+  DeviceGuard dg(m->device);
+  cudaDeviceSynchronize();
+  dfree(m->d_params);
+  dfree(m->d_grad);
+  dfree(m->d_m1);
+  dfree(m->d_m2);
+  dfree(m->d_wimg);
+  dfree(m->d_loss);
+  dfree(m->d_wsum);
+  dfree(m->d_err);
+  dfree(m->d_cells);
+  for (int f = 0; f < 6; ++f) {
+    dfree(m->feat[f]);
+    dfree(m->tgt[f]);
+    dfree(m->w[f]);
+  }
+  delete m;
+  return JXF_OK;
+}
+
+int jxf_band_set_params(jxf_band* m, const float* params) {
+  if (!m || !params) return fail(JXF_ERR_INVALID, "null argument");
+  DeviceGuard dg(m->device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(m->d_params, params, 6 * (size_t)band::kParams * 4, cudaMemcpyHostToDevice));
+  // padding entries are zero by definition (an Adam pass with lr = 0 and a zero gradient)
+  CUDA_TRY(cudaMemset(m->d_grad, 0, 6 * (size_t)band::kParams * 4));
+  band::k_band_adam<<<(6 * band::kParams + 255) / 256, 256>>>(
+      m->d_params, m->d_grad, m->d_m1, m->d_m2, 6 * band::kParams, 0.0f, 0.9f, 0.999f, 1e-8f,
+      1.0f, 1.0f);
+  CUDA_TRY(cudaMemset(m->d_m1, 0, 6 * (size_t)band::kParams * 4));
+  CUDA_TRY(cudaMemset(m->d_m2, 0, 6 * (size_t)band::kParams * 4));
+  m->adam_t = 0;
+  TRY(band_pack(m, 0));
+  CUDA_TRY(cudaDeviceSynchronize());
+  return JXF_OK;
+}
+
+int jxf_band_get_params(jxf_band* m, float* params) {
+  if (!m || !params) return fail(JXF_ERR_INVALID, "null argument");
+  DeviceGuard dg(m->device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(params, m->d_params, 6 * (size_t)band::kParams * 4, cudaMemcpyDeviceToHost));
+  return JXF_OK;
+}
+
+int jxf_band_eval(jxf_band* m, int32_t n, const float* feat, const int32_t* face, float* out) {
+  if (!m || n < 0 || (n > 0 && (!feat || !face || !out)))
+    return fail(JXF_ERR_INVALID, "invalid arguments");
+  if (n == 0) return JXF_OK;
+  for (int i = 0; i < n; ++i)
+    if (face[i] < 0 || face[i] > 5) return fail(JXF_ERR_INVALID, "face[%d] = %d", i, face[i]);
+  DeviceGuard dg(m->device);
+  std::vector<int2> per[6];
+  for (int i = 0; i < n; ++i) per[face[i]].push_back(make_int2(i, 0));
+  std::vector<int2> cells;
+  std::vector<int> tf;
+  band_tiles(per, cells, tf);
+  float* d_rows = nullptr;
+  float* d_out = nullptr;
+  int2* d_cells = nullptr;
+  int* d_tf = nullptr;
+  int64_t tally = 0;
+  int rc = dmalloc(&d_rows, (size_t)n * band::kIn, &tally);
+  if (rc == JXF_OK) rc = dmalloc(&d_out, cells.size() * band::kOut, &tally);
+  if (rc == JXF_OK) rc = upload(&d_cells, cells, &tally);
+  if (rc == JXF_OK) rc = upload(&d_tf, tf, &tally);
+  if (rc == JXF_OK &&
+      cudaMemcpy(d_rows, feat, (size_t)n * band::kIn * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(JXF_ERR_CUDA, "copy of feature rows failed");
+  if (rc == JXF_OK) {
+    band::InferArgs a{};
+    a.cells = d_cells;
+    a.tile_face = d_tf;
+    a.n_tiles = (int)tf.size();
+    a.wimg = m->d_wimg;
+    a.params = m->d_params;
+    a.delta = d_out;
+    a.rows = d_rows;
+    a.err = m->d_err;
+    a.wait_ns = wait_limit_ns();
+    band::k_band_infer<band::SRC_ROWS><<<band_ctas(a.n_tiles, m->device), 128, band::kInfSmem>>>(a);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) rc = fail(JXF_ERR_CUDA, "band eval: %s", cudaGetErrorString(e));
+  }
+  if (rc == JXF_OK) {
+    std::vector<float> h(cells.size() * band::kOut);
+    if (cudaMemcpy(h.data(), d_out, h.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = fail(JXF_ERR_CUDA, "copy of outputs failed");
+    for (size_t i = 0; rc == JXF_OK && i < cells.size(); ++i)
+      if (cells[i].x >= 0)
+        for (int o = 0; o < band::kOut; ++o) out[(size_t)cells[i].x * band::kOut + o] = h[i * 6 + o];
+  }
+  dfree(d_rows);
+  dfree(d_out);
+  dfree(d_cells);
+  dfree(d_tf);
+  if (rc == JXF_OK) rc = jxf_band_check_error(m, nullptr);
+  return rc;
+}
+
+int jxf_band_collect(jxf_band* m, float* const* fields, int32_t nx, int32_t ny, int32_t nz,
+                     const float* const* ref, int32_t rnx, int32_t rny, int32_t rnz, int32_t ox,
+                     int32_t oy, int32_t oz, void* stream) {
+  if (!m || !fields || !ref) return fail(JXF_ERR_INVALID, "null argument");
+  TRY(band_check_dims(nx, ny, nz));
+  if (ox < 0 || oy < 0 || oz < 0 || ox + nx > rnx || oy + ny > rny || oz + nz > rnz)
+    return fail(JXF_ERR_INVALID, "the %d x %d x %d box at (%d, %d, %d) is outside the %d x %d x %d "
+                "reference grid", nx, ny, nz, ox, oy, oz, rnx, rny, rnz);
+  for (int c = 0; c < 6; ++c)
+    if (!fields[c] || !ref[c]) return fail(JXF_ERR_INVALID, "null field pointer %d", c);
+  DeviceGuard dg(m->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  // earlier collects on `st` may still write the row buffers or read d_cells
+  CUDA_TRY(cudaStreamSynchronize(st));
+  std::vector<int> per[6];
+  band_cells(nx, ny, nz, per);
+  std::vector<int> all;
+  band::CollectArgs a{};
+  a.first[0] = 0;
+  for (int f = 0; f < 6; ++f) {
+    all.insert(all.end(), per[f].begin(), per[f].end());
+    a.first[f + 1] = (int)all.size();
+    TRY(band_grow(m, f, m->rows[f] + (long long)per[f].size()));
+    a.base[f] = m->rows[f];
+    a.feat[f] = m->feat[f];
+    a.tgt[f] = m->tgt[f];
+    a.w[f] = m->w[f];
+  }
+  if (all.size() > m->cells_cap) {
+    dfree(m->d_cells);
+    TRY(dmalloc(&m->d_cells, all.size(), &m->bytes));
+    m->cells_cap = all.size();
+  }
+  CUDA_TRY(cudaMemcpy(m->d_cells, all.data(), all.size() * 4, cudaMemcpyHostToDevice));
+  for (int c = 0; c < 6; ++c) {
+    a.t.f[c] = fields[c];
+    a.ref[c] = ref[c];
+  }
+  a.t.nx = nx;
+  a.t.ny = ny;
+  a.t.nz = nz;
+  a.rnx = rnx;
+  a.rny = rny;
+  a.rnz = rnz;
+  a.ox = ox;
+  a.oy = oy;
+  a.oz = oz;
+  a.cells = m->d_cells;
+  band::k_band_collect<<<((int)all.size() + 127) / 128, 128, 0, st>>>(a);
+  CUDA_TRY(cudaGetLastError());
+  for (int f = 0; f < 6; ++f) m->rows[f] += (long long)per[f].size();
+  return JXF_OK;
+}
+
+int jxf_band_dataset_size(jxf_band* m, int64_t* rows) {
+  if (!m || !rows) return fail(JXF_ERR_INVALID, "null argument");
+  for (int f = 0; f < 6; ++f) rows[f] = m->rows[f];
+  return JXF_OK;
+}
+
+int jxf_band_dataset_clear(jxf_band* m) {
+  if (!m) return fail(JXF_ERR_INVALID, "null handle");
+  for (int f = 0; f < 6; ++f) m->rows[f] = 0;
+  return JXF_OK;
+}
+
+int jxf_band_dataset_get(jxf_band* m, int32_t face, int64_t first, int64_t count, uint16_t* feat,
+                         float* target, float* weight) {
+  if (!m || face < 0 || face > 5) return fail(JXF_ERR_INVALID, "invalid handle or face");
+  if (first < 0 || count < 0 || first + count > m->rows[face])
+    return fail(JXF_ERR_INVALID, "rows [%lld, %lld) outside the %lld rows of face %d",
+                (long long)first, (long long)(first + count), m->rows[face], face);
+  if (count == 0) return JXF_OK;
+  DeviceGuard dg(m->device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  if (feat)
+    CUDA_TRY(cudaMemcpy(feat, m->feat[face] + first * band::kInP, count * band::kInP * 2,
+                        cudaMemcpyDeviceToHost));
+  if (target)
+    CUDA_TRY(cudaMemcpy(target, m->tgt[face] + first * band::kOut, count * band::kOut * 4,
+                        cudaMemcpyDeviceToHost));
+  if (weight)
+    CUDA_TRY(cudaMemcpy(weight, m->w[face] + first, count * 4, cudaMemcpyDeviceToHost));
+  return JXF_OK;
+}
+
+int jxf_band_grad(jxf_band* m, float* grad, float* loss, void* stream) {
+  if (!m) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(m->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  double ws[6];
+  TRY(band_weight_sums(m, ws, st));
+  if (m->loss_cap < 1) {
+    dfree(m->d_loss);
+    TRY(dmalloc(&m->d_loss, 6, &m->bytes));
+    m->loss_cap = 1;
+  }
+  band::TrainArgs a = band_train_args(m);
+  a.random = 0;
+  for (int f = 0; f < 6; ++f) {
+    a.tiles[f] = (int)((m->rows[f] + band::kTile - 1) / band::kTile);
+    a.scale[f] = ws[f] > 0.0 ? (float)(1.0 / ws[f]) : 0.0f;
+  }
+  a.loss = m->d_loss;
+  CUDA_TRY(cudaMemsetAsync(m->d_grad, 0, 6 * (size_t)band::kParams * 4, st));
+  CUDA_TRY(cudaMemsetAsync(m->d_loss, 0, 6 * 4, st));
+  TRY(band_train_pass(m, a, st));
+  if (grad)
+    CUDA_TRY(cudaMemcpyAsync(grad, m->d_grad, 6 * (size_t)band::kParams * 4,
+                             cudaMemcpyDeviceToHost, st));
+  if (loss) CUDA_TRY(cudaMemcpyAsync(loss, m->d_loss, 6 * 4, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return jxf_band_check_error(m, stream);
+}
+
+int jxf_band_train(jxf_band* m, int32_t iters, int32_t batch_rows, float lr, uint64_t seed,
+                   float* loss, void* stream) {
+  if (!m) return fail(JXF_ERR_INVALID, "null handle");
+  if (iters < 0 || batch_rows < 1) return fail(JXF_ERR_INVALID, "iters >= 0, batch_rows >= 1");
+  if (iters == 0) return JXF_OK;
+  DeviceGuard dg(m->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  double ws[6];
+  TRY(band_weight_sums(m, ws, st));
+  if (m->loss_cap < (size_t)iters) {
+    dfree(m->d_loss);
+    TRY(dmalloc(&m->d_loss, (size_t)iters * 6, &m->bytes));
+    m->loss_cap = (size_t)iters;
+  }
+  CUDA_TRY(cudaMemsetAsync(m->d_loss, 0, (size_t)iters * 6 * 4, st));
+  const int tiles = (batch_rows + band::kTile - 1) / band::kTile;
+  band::TrainArgs a = band_train_args(m);
+  a.random = 1;
+  for (int f = 0; f < 6; ++f) {
+    a.tiles[f] = m->rows[f] > 0 ? tiles : 0;
+    const double mean = m->rows[f] > 0 ? ws[f] / (double)m->rows[f] : 0.0;
+    a.scale[f] = mean > 0.0 ? (float)(1.0 / ((double)tiles * band::kTile * mean)) : 0.0f;
+  }
+  const float b1 = 0.9f, b2 = 0.999f;
+  for (int it = 0; it < iters; ++it) {
+    a.seed = band::mix64(seed + 0x9e3779b97f4a7c15ull * (unsigned long long)(it + 1));
+    a.loss = m->d_loss + (size_t)it * 6;
+    CUDA_TRY(cudaMemsetAsync(m->d_grad, 0, 6 * (size_t)band::kParams * 4, st));
+    TRY(band_train_pass(m, a, st));
+    m->adam_t += 1;
+    const float c1 = (float)(1.0 - std::pow(0.9, (double)m->adam_t));
+    const float c2 = (float)(1.0 - std::pow(0.999, (double)m->adam_t));
+    band::k_band_adam<<<(6 * band::kParams + 255) / 256, 256, 0, st>>>(
+        m->d_params, m->d_grad, m->d_m1, m->d_m2, 6 * band::kParams, lr, b1, b2, 1e-8f, c1, c2);
+    TRY(band_pack(m, st));
+  }
+  CUDA_TRY(cudaGetLastError());
+  if (loss) {
+    std::vector<float> h((size_t)iters * 6);
+    CUDA_TRY(cudaMemcpyAsync(h.data(), m->d_loss, h.size() * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int it = 0; it < iters; ++it) {
+      float s = 0.0f;
+      for (int f = 0; f < 6; ++f) s += h[(size_t)it * 6 + f];
+      loss[it] = s;
+    }
+  }
+  return jxf_band_check_error(m, stream);
+}
+
+int jxf_band_check_error(jxf_band* m, void* stream) {
+  if (!m) return fail(JXF_ERR_INVALID, "null handle");
+  DeviceGuard dg(m->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int h[4] = {0, 0, 0, 0};
+  CUDA_TRY(cudaMemcpyAsync(h, m->d_err, 16, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  CUDA_TRY(cudaGetLastError());
+  if (h[0] != 0) {
+    CUDA_TRY(cudaMemsetAsync(m->d_err, 0, 16, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return fail(JXF_ERR_TIMEOUT,
+                "a tensor-core step did not complete within the wait limit (code 0x%x, block %d, "
+                "face %d, thread %d)",
+                h[0], h[1], h[2], h[3]);
+  }
+  return JXF_OK;
+}
+
+int jxf_batch3d_set_band(jxf_batch3d* b, jxf_band* m) {
+  if (!b) return fail(JXF_ERR_INVALID, "null batch");
+  DeviceGuard dg(b->device);
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->band = nullptr;
+  b->band_tiles = 0;
+  if (!m) return JXF_OK;
+  if (m->device != b->device) return fail(JXF_ERR_INVALID, "band and batch on different devices");
+  std::vector<band::GridRef> refs;
+  std::vector<int2> per[6];
+  std::vector<int> cells[6];
+  for (size_t k = 0; k < b->grids.size(); ++k) {
+    jxf_grid3d* g = b->grids[k];
+    if (g->d.boundary != JXF_BND_PEC)
+      return fail(JXF_ERR_INVALID, "grid %zu: a learned band needs PEC-walled grids", k);
+    TRY(band_check_dims(g->d.nx, g->d.ny, g->d.nz));
+    band::GridRef r{};
+    for (int c = 0; c < 6; ++c) r.f[c] = g->f[0][c];
+    r.nx = g->d.nx;
+    r.ny = g->d.ny;
+    r.nz = g->d.nz;
+    refs.push_back(r);
+    band_cells(g->d.nx, g->d.ny, g->d.nz, cells);
+    for (int f = 0; f < 6; ++f)
+      for (int c : cells[f]) per[f].push_back(make_int2(c, (int)k));
+  }
+  std::vector<int2> tc;
+  std::vector<int> tf;
+  band_tiles(per, tc, tf);
+  dfree(b->d_band_grids);
+  dfree(b->d_band_cells);
+  dfree(b->d_band_tile_face);
+  dfree(b->d_band_delta);
+  TRY(upload(&b->d_band_grids, refs, &b->bytes));
+  TRY(upload(&b->d_band_cells, tc, &b->bytes));
+  TRY(upload(&b->d_band_tile_face, tf, &b->bytes));
+  TRY(dmalloc(&b->d_band_delta, tc.size() * band::kOut, &b->bytes));
+  b->band_tiles = (int)tf.size();
+  b->band_ctas = band_ctas(b->band_tiles, b->device);
+  b->band = m;
+  return JXF_OK;
+}
+
+}  // extern "C"
 
 // ---------------------------------------------------------------------------
 // Adjoint (permittivity gradients of probe objectives)

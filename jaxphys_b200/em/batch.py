@@ -35,6 +35,14 @@ class FDTDBatch:
         nat.check(lib.jxf_batch3d_create(len(grids), arr, C.byref(h)), "jxf_batch3d_create")
         self._h = h
         self._last_n = 0
+        self.band = None
+
+    def set_band(self, model) -> None:
+        """Attach a learned absorbing band (``LearnedBand``; PEC grids only)
+        applied after every step; ``None`` detaches it."""
+        nat.check(nat.load().jxf_batch3d_set_band(self._h, None if model is None else model._h),
+                  "jxf_batch3d_set_band")
+        self.band = model
 
     def close(self):
         if self._h is not None:

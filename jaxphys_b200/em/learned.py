@@ -1,0 +1,351 @@
+"""Learned absorbing band (extension): a per-cell MLP boundary a few cells thick.
+
+A PEC-walled grid whose outer 3 cell layers form the band.  After every
+plain Yee step, each cell of the outer layer is corrected by one small
+network per face (54 -> 64 -> 64 -> 6, tanh-form GELU, BF16 weights with
+FP32 accumulation on the tensor cores, C ABI ``jxf_band_*``):
+
+    X_c <- X_c + s * net_f(v / s)
+
+where v is the 3 x 3 stencil (3 band layers along the face normal x -1, 0, +1
+along the face's first tangent axis) of the six components (H scaled by
+eta0) and s its RMS.  The networks are trained on the GPU by the engine's own
+forward/backward kernels against traces of plain 16-layer CPML runs on padded
+domains: for a reference state at step n, the truncated grid takes one plain
+step and the target is the reference's state at n + 1 (``collect_traces``).
+
+``LearnedBand``       the 6-face model (parameters, training, evaluation)
+``BandCase``          one training / evaluation problem (interior box,
+                      permittivity, sources)
+``collect_traces``    training rows from padded CPML reference runs
+``reflection_db``     boundary error of learned / CPML / bare-PEC runs
+                      against a padded reference, in dB
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .. import _native as nat
+from ..exceptions import ConfigurationError, SimulationError
+from .fdtd3d import COMPONENTS, CPMLSpec, EMGrid3D, PointSource3D
+
+N_PARAMS = nat.BAND_PARAMS
+N_FACES = nat.BAND_FACES
+N_FEATURES = nat.BAND_FEATURES
+BAND_LAYERS = 3
+
+
+def _pad_mask() -> np.ndarray:
+    m = np.zeros(N_PARAMS, dtype=bool)
+    w1 = slice(0, 64 * 64)
+    m[w1] = (np.arange(64 * 64) % 64) >= N_FEATURES
+    w3 = 64 * 64 + 64 + 64 * 64 + 64
+    m[w3:w3 + 16 * 64] = (np.arange(16 * 64) // 64) >= 6
+    m[w3 + 16 * 64:] = np.arange(16) >= 6
+    return m
+
+
+def init_params(seed: int = 0, out_scale: float = 0.1) -> np.ndarray:
+    """He-style initial parameters [6, N_PARAMS] (padding entries zero)."""
+    rng = np.random.default_rng(seed)
+    P = np.zeros((N_FACES, N_PARAMS), dtype=np.float32)
+    for f in range(N_FACES):
+        w1 = P[f, :4096].reshape(64, 64)
+        w2 = P[f, 4160:8256].reshape(64, 64)
+        w3 = P[f, 8320:9344].reshape(16, 64)
+        w1[:, :N_FEATURES] = rng.normal(0, math.sqrt(2.0 / N_FEATURES), (64, N_FEATURES))
+        w2[:] = rng.normal(0, math.sqrt(2.0 / 64), (64, 64))
+        w3[:6] = rng.normal(0, out_scale / 8.0, (6, 64))
+    return P
+
+
+def _field_ptrs(g: EMGrid3D):
+    lib = nat.load()
+    out = (C.c_void_p * 6)()
+    for c in range(6):
+        p = C.c_void_p()
+        nat.check(lib.jxf_grid3d_field_ptr(g._h, c, C.byref(p)), "field_ptr")
+        out[c] = p.value
+    return out
+
+
+class LearnedBand:
+    """The six per-face networks of a learned absorbing band on one GPU."""
+
+    def __init__(self, params: np.ndarray | None = None, *, seed: int = 0,
+                 device: int | None = None):
+        import torch
+
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        h = C.c_void_p()
+        nat.check(nat.load().jxf_band_create(self.device, C.byref(h)), "jxf_band_create")
+        self._h = h
+        self.params = init_params(seed) if params is None else params
+
+    def close(self) -> None:
+        if self._h is not None:
+            nat.load().jxf_band_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.empty((N_FACES, N_PARAMS), dtype=np.float32)
+        nat.check(nat.load().jxf_band_get_params(self._h, out.ctypes.data), "get_params")
+        return out
+
+    @params.setter
+    def params(self, p) -> None:
+        p = np.ascontiguousarray(np.asarray(p, dtype=np.float32))
+        if p.shape != (N_FACES, N_PARAMS):
+            raise ConfigurationError(f"params must have shape {(N_FACES, N_PARAMS)}")
+        nat.check(nat.load().jxf_band_set_params(self._h, p.ctypes.data), "set_params")
+
+    def save(self, path) -> None:
+        np.savez(path, params=self.params)
+
+    @classmethod
+    def load(cls, path, device: int | None = None) -> "LearnedBand":
+        with np.load(path) as z:
+            return cls(z["params"], device=device)
+
+    # ---------------------------------------------------------------- eval
+    def eval(self, feat, face) -> np.ndarray:
+        """Network outputs [n, 6] for normalised feature rows [n, 54]."""
+        x = np.ascontiguousarray(np.asarray(feat, dtype=np.float32))
+        f = np.ascontiguousarray(np.asarray(face, dtype=np.int32))
+        if x.ndim != 2 or x.shape[1] != N_FEATURES or f.shape != (x.shape[0],):
+            raise ConfigurationError("feat must be [n, 54] and face [n]")
+        out = np.empty((x.shape[0], 6), dtype=np.float32)
+        nat.check(nat.load().jxf_band_eval(self._h, x.shape[0], x.ctypes.data, f.ctypes.data,
+                                           out.ctypes.data), "jxf_band_eval")
+        return out
+
+    # ------------------------------------------------------------ dataset
+    def collect(self, grid: EMGrid3D, ref: EMGrid3D, offset) -> None:
+        """Append rows for ``grid``'s outer cells against ``ref``'s state
+        (the box of ``grid``'s size at ``offset`` in ``ref``)."""
+        ox, oy, oz = (int(v) for v in offset)
+        nx, ny, nz = grid.size
+        rx, ry, rz = ref.size
+        nat.check(nat.load().jxf_band_collect(self._h, _field_ptrs(grid), nx, ny, nz,
+                                              _field_ptrs(ref), rx, ry, rz, ox, oy, oz,
+                                              nat.stream_handle()), "jxf_band_collect")
+
+    def dataset_size(self) -> np.ndarray:
+        out = np.zeros(N_FACES, dtype=np.int64)
+        nat.check(nat.load().jxf_band_dataset_size(self._h, out.ctypes.data), "dataset_size")
+        return out
+
+    def clear(self) -> None:
+        nat.check(nat.load().jxf_band_dataset_clear(self._h), "dataset_clear")
+
+    def dataset(self, face: int, first: int = 0, count: int | None = None):
+        """(features float32 [m, 64] as stored in BF16, targets [m, 6], weights [m])."""
+        n = int(self.dataset_size()[face])
+        count = n - first if count is None else int(count)
+        bits = np.empty((count, 64), dtype=np.uint16)
+        tgt = np.empty((count, 6), dtype=np.float32)
+        w = np.empty(count, dtype=np.float32)
+        nat.check(nat.load().jxf_band_dataset_get(self._h, int(face), int(first), count,
+                                                  bits.ctypes.data, tgt.ctypes.data,
+                                                  w.ctypes.data), "dataset_get")
+        feat = (bits.astype(np.uint32) << 16).view(np.float32)
+        return feat, tgt, w
+
+    # ------------------------------------------------------------ training
+    def grad(self):
+        """(gradient [6, N_PARAMS], loss [6]) over the whole dataset."""
+        g = np.empty((N_FACES, N_PARAMS), dtype=np.float32)
+        loss = np.empty(N_FACES, dtype=np.float32)
+        nat.check(nat.load().jxf_band_grad(self._h, g.ctypes.data, loss.ctypes.data,
+                                           nat.stream_handle()), "jxf_band_grad")
+        return g, loss
+
+    def train(self, iters: int, batch_rows: int = 8192, lr: float = 1e-3,
+              seed: int = 0) -> np.ndarray:
+        """Adam steps on random rows (batch_rows per face); per-step loss."""
+        loss = np.empty(max(int(iters), 0), dtype=np.float32)
+        nat.check(nat.load().jxf_band_train(self._h, int(iters), int(batch_rows), float(lr),
+                                            int(seed) & 0xFFFFFFFFFFFFFFFF, loss.ctypes.data,
+                                            nat.stream_handle()), "jxf_band_train")
+        return loss
+
+    def check(self) -> None:
+        nat.check(nat.load().jxf_band_check_error(self._h, nat.stream_handle()), "band")
+
+
+# ---------------------------------------------------------------------------
+# problems, training traces and reflection measurement
+
+
+@dataclass
+class BandCase:
+    """An interior box with its permittivity and sources (interior coordinates)."""
+
+    size: tuple[int, int, int]
+    eps: np.ndarray | None = None
+    sources: list = field(default_factory=list)
+
+    def grid(self, pad: int, boundary: str, pml_layers: int = 0, resolution: float = 1.0,
+             path: str = "generic", cpml: CPMLSpec | None = None) -> EMGrid3D:
+        """This case embedded with `pad` vacuum cells on every side."""
+        n = tuple(int(v) + 2 * pad for v in self.size)
+        g = EMGrid3D(n, resolution=resolution, boundary=boundary, pml_layers=pml_layers,
+                     cpml=cpml, path=path)
+        if self.eps is not None:
+            eps = np.ones(n, dtype=np.float32)
+            sx, sy, sz = self.size
+            eps[pad:pad + sx, pad:pad + sy, pad:pad + sz] = self.eps
+            g.set_permittivity(eps)
+        for s in self.sources:
+            x, y, z = s.position
+            g.add_source(PointSource3D(frequency=s.frequency, position=(x + pad, y + pad, z + pad),
+                                       amplitude=s.amplitude, polarization=s.polarization,
+                                       waveform=s.waveform, width_steps=s.width_steps,
+                                       delay_steps=s.delay_steps))
+        return g
+
+
+def smooth_eps(rng: np.random.Generator, shape, lo: float, hi: float,
+               sigma: float = 4.0) -> np.ndarray:
+    """Gaussian-smoothed uniform noise rescaled to [lo, hi] (float32)."""
+    from scipy.ndimage import gaussian_filter
+
+    a = gaussian_filter(rng.random(shape), sigma, mode="nearest")
+    a = (a - a.min()) / max(float(a.max() - a.min()), 1e-12)
+    return (lo + (hi - lo) * a).astype(np.float32)
+
+
+def random_case(rng: np.random.Generator, size, eps_range=(1.0, 6.0), n_sources: int = 1,
+                margin: int = 4, dt_freq: float = 0.05, width: float = 30.0,
+                resolution: float = 1.0) -> BandCase:
+    """Random smoothed permittivity and dipoles (random position / orientation)
+    driven by a Gaussian-modulated sinusoid of centre frequency dt_freq / dt."""
+    size = tuple(int(v) for v in size)
+    dt = 0.99 * resolution / (299792458.0 * math.sqrt(3.0))
+    eps = smooth_eps(rng, size, *eps_range) if eps_range[1] > eps_range[0] else None
+    srcs = []
+    for _ in range(n_sources):
+        pos = tuple(int(rng.integers(margin, s - margin)) for s in size)
+        srcs.append(PointSource3D(frequency=dt_freq / dt, position=pos,
+                                  polarization=str(rng.choice(["x", "y", "z"])),
+                                  waveform="gauss_sine", width_steps=width))
+    return BandCase(size, eps, srcs)
+
+
+def _copy_box(dst: EMGrid3D, src: EMGrid3D, off) -> None:
+    ox, oy, oz = off
+    nx, ny, nz = dst.size
+    for name in COMPONENTS:
+        dst.set_field(name, src.field(name)[ox:ox + nx, oy:oy + ny, oz:oz + nz].contiguous())
+
+
+def collect_traces(model: LearnedBand, case: BandCase, n_steps: int, every: int = 2,
+                   start: int = 0, ref_pml: int = 16, resolution: float = 1.0) -> None:
+    """Training rows for `case` (band grid = interior + 3 vacuum layers per side).
+
+    The padded reference grid adds `ref_pml` CPML layers around the band grid.
+    Every `every` steps from `start`, the band grid is loaded with the
+    reference state, takes one plain (PEC) step, and its outer cells are
+    compared with the reference one step later.
+    """
+    ref = case.grid(BAND_LAYERS + ref_pml, "cpml", ref_pml, resolution, path="auto")
+    trunc = BandCase(case.size, case.eps, []).grid(BAND_LAYERS, "pec", 0, resolution)
+    ref.prepare()
+    trunc.prepare(ref._dt)
+    off = (ref_pml, ref_pml, ref_pml)
+    for n in range(int(n_steps)):
+        if n >= start and (n - start) % every == 0:
+            _copy_box(trunc, ref, off)
+            trunc.step(1)
+            ref.step(1)
+            model.collect(trunc, ref, off)
+        else:
+            ref.step(1)
+    ref.check()
+    model.check()
+    ref._release()
+    trunc._release()
+
+
+def reflection_db(case: BandCase, n_steps: int, model: LearnedBand | None = None,
+                  cpml_layers: tuple = (10,), ref_pml: int = 16, every: int = 10,
+                  resolution: float = 1.0, pec: bool = True) -> dict:
+    """Boundary error of each method against a padded CPML reference, in dB:
+
+        20 log10( ||E - E_ref|| / ||E_ref|| )
+
+    over the interior box and the steps every, 2 every, ... (E = Ex, Ey, Ez).
+    Methods: "learned" (band of 3 layers, `model`), "pec" (the same grid
+    without the band), "cpml<k>" (k-layer CPML around the interior).
+    """
+    import torch
+
+    from .batch import FDTDBatch
+
+    runs = {}
+    pad_ref = max(BAND_LAYERS, max(cpml_layers) if cpml_layers else 0) + ref_pml
+    ref = case.grid(pad_ref, "cpml", ref_pml, resolution, path="auto")
+    ref.prepare()
+    dt = ref._dt
+    if model is not None:
+        g = case.grid(BAND_LAYERS, "pec", 0, resolution)
+        g.prepare(dt)
+        b = FDTDBatch([g])
+        b.set_band(model)
+        runs["learned"] = (g, BAND_LAYERS, b)
+    if pec:
+        g = case.grid(BAND_LAYERS, "pec", 0, resolution)
+        g.prepare(dt)
+        runs["pec"] = (g, BAND_LAYERS, None)
+    for k in cpml_layers:
+        g = case.grid(k, "cpml", k, resolution, path="auto")
+        g.prepare(dt)
+        runs[f"cpml{k}"] = (g, k, None)
+    num = {k: 0.0 for k in runs}
+    den = 0.0
+    sx, sy, sz = case.size
+
+    def interior(g, off):
+        return torch.stack([g.field(c)[off:off + sx, off:off + sy, off:off + sz]
+                            for c in ("ex", "ey", "ez")]).double()
+
+    done = 0
+    while done < n_steps:
+        k = min(every, n_steps - done)
+        ref.step(k)
+        for name, (g, off, b) in runs.items():
+            if b is not None:
+                b.run(k, use_graph=False)
+            else:
+                g.step(k)
+        done += k
+        e_ref = interior(ref, pad_ref)
+        den += float((e_ref * e_ref).sum())
+        for name, (g, off, b) in runs.items():
+            d = interior(g, off) - e_ref
+            num[name] += float((d * d).sum())
+    out = {}
+    for name, (g, off, b) in runs.items():
+        if not math.isfinite(num[name]):
+            out[name] = float("inf")
+        else:
+            out[name] = 10.0 * math.log10(max(num[name], 1e-300) / max(den, 1e-300))
+        if b is not None:
+            b.close()
+        g._release()
+    ref._release()
+    if model is not None:
+        model.check()
+    return out
