@@ -1868,14 +1868,22 @@ int band_launch(jxf_band* m, const band::GridRef* grids, const int2* cells, cons
   return JXF_OK;
 }
 
-// CTAs of the inference kernel: resident CTAs per SM (at most 4, which also
-// keeps 4 x 128 TMEM columns within the SM's 512) times the SM count.
+// CTAs of the inference kernel: resident CTAs per SM (limited by shared
+// memory, registers and the SM's 512 TMEM columns) times the SM count.
 int band_ctas(int n_tiles, int device) {
-  int sms = 148, occ = 1;
+  int sms = 148, smem_sm = 233472, regs_sm = 65536;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, band::k_band_infer<band::SRC_GRIDS>, 128,
-                                                band::kInfSmem);
-  occ = std::max(1, std::min(occ, 4));
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+  cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device);
+  cudaFuncAttributes fa{};
+  int regs = 128;
+  if (cudaFuncGetAttributes(&fa, band::k_band_infer<band::SRC_GRIDS>) == cudaSuccess)
+    regs = std::max(fa.numRegs, 1);
+  cudaGetLastError();
+  const int by_smem = smem_sm / (band::kInfSmem + 1024);
+  const int by_regs = regs_sm / (regs * 128);
+  const int by_tmem = 512 / band::kInfTmemCols;
+  const int occ = std::max(1, std::min(std::min(by_smem, by_regs), by_tmem));
   return std::max(1, std::min(n_tiles, sms * occ));
 }
 

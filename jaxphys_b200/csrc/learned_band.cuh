@@ -37,14 +37,19 @@ constexpr int kB2 = kW2 + kHid * kHid;      // [64]
 constexpr int kW3 = kB2 + kHid;             // [16][64] (out, in), out >= 6 zero
 constexpr int kB3 = kW3 + kOutP * kHid;     // [16], >= 6 zero
 constexpr int kParams = kB3 + kOutP;        // 9360
+// Biases ride in the MMA: the input tile carries a constant 1 in column 54
+// (an unused input), the hidden tiles in column 64 of a K = 80 image, and the
+// weight images hold the BF16 bias in that column.
+constexpr int kOneX = 54;
+constexpr int kKH = 80;                     // K of the hidden-activation images
 // BF16 operand images of one face (bytes).
-constexpr int kImgW1 = 0;          // W1, 64 x 64, K = in
-constexpr int kImgW2 = 8192;       // W2, 64 x 64, K = in
-constexpr int kImgW3 = 16384;      // W3, 16 x 64, K = in
-constexpr int kImgW2T = 18432;     // W2^T, 64 x 64, K = out
-constexpr int kImgW3T = 26624;     // W3^T, 64 x 16, K = out
-constexpr int kImgBytes = 28672;
-constexpr int kImgFwdBytes = 18432;  // W1, W2, W3
+constexpr int kImgW1 = 0;          // W1 | b1 at column 54, 64 x 64
+constexpr int kImgW2 = 8192;       // W2 | b2 at column 64, 64 x 80
+constexpr int kImgW3 = 18432;      // W3 | b3 at column 64, 16 x 80
+constexpr int kImgFwdBytes = 20992;
+constexpr int kImgW2T = 20992;     // W2^T, 64 x 64 (K = out)
+constexpr int kImgW3T = 29184;     // W3^T, 64 x 16 (K = out)
+constexpr int kImgBytes = 31232;
 constexpr float kEta0 = 376.730313668f;
 constexpr int kTile = 128;
 
@@ -68,19 +73,90 @@ __device__ __forceinline__ float tanh_fast(float x) {
 }
 constexpr float kGeluC0 = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float kGeluC1 = 0.044715f;
-__device__ __forceinline__ float gelu(float x) {
-  const float t = tanh_fast(kGeluC0 * fmaf(kGeluC1 * x, x * x, x));
-  return 0.5f * x * (1.0f + t);
+
+// GELU of two values in packed BF16 arithmetic (the activation is a BF16
+// MMA operand anyway): x rounded to BF16, then
+//   g = h + h tanh(x (c0 + c0 c1 x^2)),  h = x / 2,
+// every product / FMA rounded to BF16, tanh by tanh.approx.bf16x2.
+__device__ __forceinline__ uint32_t gelu2(float x0, float x1) {
+  const __nv_bfloat162 x = __floats2bfloat162_rn(x0, x1);
+  const __nv_bfloat162 c0 = __float2bfloat162_rn(kGeluC0);
+  const __nv_bfloat162 c01 = __float2bfloat162_rn(kGeluC0 * kGeluC1);
+  const __nv_bfloat162 half = __float2bfloat162_rn(0.5f);
+  const __nv_bfloat162 p = __hfma2(__hmul2(x, x), c01, c0);
+  const __nv_bfloat162 u = __hmul2(x, p);
+  uint32_t ub = *reinterpret_cast<const uint32_t*>(&u), tb;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tb) : "r"(ub));
+  const __nv_bfloat162 t = *reinterpret_cast<const __nv_bfloat162*>(&tb);
+  const __nv_bfloat162 h = __hmul2(x, half);
+  const __nv_bfloat162 g = __hfma2(h, t, h);
+  return *reinterpret_cast<const uint32_t*>(&g);
 }
+// d GELU / dx of the tanh form, FP32 (training backward).
 __device__ __forceinline__ float gelu_grad(float x) {
   const float x2 = x * x;
-  const float t = tanh_fast(kGeluC0 * fmaf(kGeluC1 * x, x2, x));
+  const float t = tanh_fast(x * fmaf(kGeluC0 * kGeluC1, x2, kGeluC0));
   return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluC0 * fmaf(3.0f * kGeluC1, x2, 1.0f);
+}
+
+// Store 64 packed-BF16 values (32 words) as row r of a K-column image.
+__device__ __forceinline__ void put_row_packed(unsigned char* img, int r, const uint32_t* w,
+                                               int K) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    *reinterpret_cast<uint4*>(img + tc::img_off(r, 8 * c, K)) =
+        make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+}
+// Store 64 FP32 values rounded to BF16 as row r of a K-column image.
+__device__ __forceinline__ void put_row_f32(unsigned char* img, int r, const float* v, int K) {
+  uint32_t w[32];
+#pragma unroll
+  for (int c = 0; c < 32; ++c) w[c] = tc::pack_bf16(v[2 * c], v[2 * c + 1]);
+  put_row_packed(img, r, w, K);
+}
+// Column r (sample r) of a 64 x 128 image from 64 packed-BF16 values.
+__device__ __forceinline__ void put_col_packed(unsigned char* imgT, int r, const uint32_t* w) {
+#pragma unroll
+  for (int q = 0; q < 32; ++q) {
+    *reinterpret_cast<uint16_t*>(imgT + tc::img_off(2 * q, r, 128)) = (uint16_t)(w[q] & 0xFFFFu);
+    *reinterpret_cast<uint16_t*>(imgT + tc::img_off(2 * q + 1, r, 128)) = (uint16_t)(w[q] >> 16);
+  }
+}
+// Constant tail of a 128 x 80 hidden image: column 64 = 1, 65..79 = 0.
+__device__ __forceinline__ void init_hidden_tail(unsigned char* img, int tid, int nthreads) {
+  for (int r = tid; r < kTile; r += nthreads) {
+    *reinterpret_cast<uint4*>(img + tc::img_off(r, 64, kKH)) = make_uint4(0x3F80u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(img + tc::img_off(r, 72, kKH)) = make_uint4(0u, 0u, 0u, 0u);
+  }
 }
 
 // Raw stencil of an outer cell (v[54], H scaled by eta0); returns s.
 __device__ __forceinline__ float gather(const GridRef& g, int cell, int face, float* v) {
   const int a = face >> 1, side = face & 1;
+  float ss = 0.0f;
+  if (a == 2 && (g.nz & 3) == 0) {
+    // z faces: the three band layers of a row are one aligned 16-byte load
+    const long long row = (long long)cell - (side ? g.nz - 1 : 0) + (side ? g.nz - 4 : 0);
+    const int x = cell / (g.nz * g.ny);
+    const long long sx = (long long)g.ny * g.nz;
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+      const bool in = x + w - 1 >= 0 && x + w - 1 < g.nx;
+#pragma unroll
+      for (int comp = 0; comp < 6; ++comp) {
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (in) q = __ldg(reinterpret_cast<const float4*>(g.f[comp] + row + (w - 1) * sx));
+        const float sc = comp >= 3 ? kEta0 : 1.0f;
+        const float l0 = (side ? q.w : q.x) * sc, l1 = (side ? q.z : q.y) * sc,
+                    l2 = (side ? q.y : q.z) * sc;
+        v[comp * 9 + 0 * 3 + w] = l0;
+        v[comp * 9 + 1 * 3 + w] = l1;
+        v[comp * 9 + 2 * 3 + w] = l2;
+        ss = fmaf(l0, l0, fmaf(l1, l1, fmaf(l2, l2, ss)));
+      }
+    }
+    return sqrtf(ss * (1.0f / kIn) + 1e-30f);
+  }
   const int t1 = a == 2 ? 0 : a + 1;
   const int z = cell % g.nz;
   const int y = (cell / g.nz) % g.ny;
@@ -90,7 +166,6 @@ __device__ __forceinline__ float gather(const GridRef& g, int cell, int face, fl
   const long long st = t1 == 0 ? sx : (t1 == 1 ? (long long)g.nz : 1ll);
   const int ct = t1 == 0 ? x : (t1 == 1 ? y : z);
   const int nt = t1 == 0 ? g.nx : (t1 == 1 ? g.ny : g.nz);
-  float ss = 0.0f;
 #pragma unroll
   for (int l = 0; l < 3; ++l) {
     const long long dn = side ? -l * sa : l * sa;
@@ -110,10 +185,20 @@ __device__ __forceinline__ float gather(const GridRef& g, int cell, int face, fl
   return sqrtf(ss * (1.0f / kIn) + 1e-30f);
 }
 
+// All threads wait for `bar`; false (for every thread) if any timed out.
+__device__ __forceinline__ bool wait_all(uint64_t* bar, uint32_t phase, unsigned long long ns,
+                                        int* err, int where) {
+  const bool ok = mbar_wait_bounded(bar, phase, ns);
+  if (!ok) report_error(err, ERR_TIMEOUT_BASE | 0x100 | where, blockIdx.x, blockIdx.y, threadIdx.x);
+  return __syncthreads_or(!ok) == 0;
+}
+
 // ---------------------------------------------------------------------------
 // Inference (tensor cores).  One CTA = 4 warps; thread t owns row t of each
 // 128-cell tile.  Tiles are single-face; a CTA works through a contiguous
-// range of tiles and reloads the face's weights when the face changes.
+// range of tiles and reloads the face's weights when the face changes.  One
+// activation image (X, then G1, then G2; each MMA has completed before the
+// next epilogue overwrites it) and 64 TMEM columns (Z1, then Z2, then O).
 enum InferSrc : int { SRC_GRIDS = 0, SRC_ROWS = 1 };
 
 struct InferArgs {
@@ -129,29 +214,17 @@ struct InferArgs {
   unsigned long long wait_ns;
 };
 
-constexpr int kInfOffX = 0;        // X, then G2 (128 x 64)
-constexpr int kInfOffG1 = 16384;   // G1 (128 x 64)
-constexpr int kInfOffW = 32768;    // W1 | W2 | W3
-constexpr int kInfOffB = kInfOffW + kImgFwdBytes;   // biases b1 | b2 | b3 (144 floats)
-constexpr int kInfOffBar = kInfOffB + 144 * 4;
+constexpr int kInfOffA = 0;        // activation image, 128 x 80
+constexpr int kInfOffW = 20480;    // W1 | W2 | W3 images
+constexpr int kInfOffBar = kInfOffW + kImgFwdBytes;
 constexpr int kInfSmem = kInfOffBar + 16;
-constexpr int kInfTmemCols = 128;
-
-// All threads wait for `bar`; false (for every thread) if any timed out.
-__device__ __forceinline__ bool wait_all(uint64_t* bar, uint32_t phase, unsigned long long ns,
-                                        int* err, int where) {
-  const bool ok = mbar_wait_bounded(bar, phase, ns);
-  if (!ok) report_error(err, ERR_TIMEOUT_BASE | 0x100 | where, blockIdx.x, blockIdx.y, threadIdx.x);
-  return __syncthreads_or(!ok) == 0;
-}
+constexpr int kInfTmemCols = 64;
 
 template <int SRC>
 __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ InferArgs p) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* bufX = smem + kInfOffX;
-  unsigned char* bufG1 = smem + kInfOffG1;
+  unsigned char* bufA = smem + kInfOffA;
   unsigned char* bufW = smem + kInfOffW;
-  float* bias = reinterpret_cast<float*>(smem + kInfOffB);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kInfOffBar);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kInfOffBar + 8);
   const int tid = threadIdx.x;
@@ -162,6 +235,7 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
     mbar_init(bar, 1);
     fence_barrier_init();
   }
+  init_hidden_tail(bufA, tid, 128);
   if (tid < 32) {
     tc::tmem_alloc(tslot, kInfTmemCols);
     tc::tmem_relinquish();
@@ -171,7 +245,7 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
   tc::fence_after_sync();
   const uint32_t tm = *tslot;
   const uint32_t lane_base = tc::taddr(tm, (tid >> 5) * 32, 0);
-  const uint32_t sX = smem_u32(bufX), sG1 = smem_u32(bufG1), sW = smem_u32(bufW);
+  const uint32_t sA = smem_u32(bufA), sW = smem_u32(bufW);
   constexpr uint32_t id64 = tc::idesc_bf16(128, 64), id16 = tc::idesc_bf16(128, 16);
   uint32_t phase = 0;
   int cur_face = -1;
@@ -182,9 +256,6 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
       const uint4* src = reinterpret_cast<const uint4*>(p.wimg + (size_t)face * kImgBytes);
       uint4* dst = reinterpret_cast<uint4*>(bufW);
       for (int k = tid; k < kImgFwdBytes / 16; k += 128) dst[k] = __ldg(src + k);
-      const float* pf = p.params + (size_t)face * kParams;
-      for (int k = tid; k < 144; k += 128)
-        bias[k] = k < 64 ? pf[kB1 + k] : (k < 128 ? pf[kB2 + k - 64] : pf[kB3 + k - 128]);
       cur_face = face;
     }
     const int i = t * kTile + tid;
@@ -206,58 +277,70 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
 #pragma unroll
       for (int k = 0; k < kIn; ++k) v[k] = 0.0f;
     }
+    v[kOneX] = 1.0f;
 #pragma unroll
-    for (int k = kIn; k < kInP; ++k) v[k] = 0.0f;
-    tc::put_row64(bufX, tid, v);
+    for (int k = kOneX + 1; k < kInP; ++k) v[k] = 0.0f;
+    put_row_f32(bufA, tid, v, kKH);
     fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
-    // layer 1: Z1 = X W1^T  (TMEM columns 0..63)
+    // layer 1: Z1 = [X 1] [W1 b1]^T
     if (tid == 0) {
       tc::fence_after_sync();
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk)
-        tc::mma(tm, tc::img_desc(sX, 64, kk), tc::img_desc(sW + kImgW1, 64, kk), id64, kk);
+        tc::mma(tm, tc::img_desc(sA, kKH, kk), tc::img_desc(sW + kImgW1, 64, kk), id64, kk);
       tc::commit(bar);
     }
     ok = wait_all(bar, phase, p.wait_ns, p.err, 1);
     phase ^= 1;
     if (!ok) break;
     tc::fence_after_sync();
-    tc::ld32(lane_base, v);
-    tc::ld32(lane_base + 32, v + 32);
+    uint32_t g[32];
+    {
+      float z[32];
 #pragma unroll
-    for (int k = 0; k < kHid; ++k) v[k] = gelu(v[k] + bias[k]);
-    tc::put_row64(bufG1, tid, v);
+      for (int hlf = 0; hlf < 2; ++hlf) {
+        tc::ld32(lane_base + 32 * hlf, z);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) g[16 * hlf + c] = gelu2(z[2 * c], z[2 * c + 1]);
+      }
+    }
+    put_row_packed(bufA, tid, g, kKH);
     fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
-    // layer 2: Z2 = G1 W2^T  (columns 64..127)
+    // layer 2: Z2 = [G1 1] [W2 b2]^T
     if (tid == 0) {
       tc::fence_after_sync();
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk)
-        tc::mma(tm + 64, tc::img_desc(sG1, 64, kk), tc::img_desc(sW + kImgW2, 64, kk), id64, kk);
+      for (int kk = 0; kk < 5; ++kk)
+        tc::mma(tm, tc::img_desc(sA, kKH, kk), tc::img_desc(sW + kImgW2, kKH, kk), id64, kk);
       tc::commit(bar);
     }
     ok = wait_all(bar, phase, p.wait_ns, p.err, 2);
     phase ^= 1;
     if (!ok) break;
     tc::fence_after_sync();
-    tc::ld32(lane_base + 64, v);
-    tc::ld32(lane_base + 64 + 32, v + 32);
+    {
+      float z[32];
 #pragma unroll
-    for (int k = 0; k < kHid; ++k) v[k] = gelu(v[k] + bias[64 + k]);
-    tc::put_row64(bufX, tid, v);  // G2 over X (layer 1 is complete)
+      for (int hlf = 0; hlf < 2; ++hlf) {
+        tc::ld32(lane_base + 32 * hlf, z);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) g[16 * hlf + c] = gelu2(z[2 * c], z[2 * c + 1]);
+      }
+    }
+    put_row_packed(bufA, tid, g, kKH);
     fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
-    // layer 3: O = G2 W3^T  (columns 0..15)
+    // layer 3: O = [G2 1] [W3 b3]^T  (columns 0..15)
     if (tid == 0) {
       tc::fence_after_sync();
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk)
-        tc::mma(tm, tc::img_desc(sX, 64, kk), tc::img_desc(sW + kImgW3, 64, kk), id16, kk);
+      for (int kk = 0; kk < 5; ++kk)
+        tc::mma(tm, tc::img_desc(sA, kKH, kk), tc::img_desc(sW + kImgW3, kKH, kk), id16, kk);
       tc::commit(bar);
     }
     ok = wait_all(bar, phase, p.wait_ns, p.err, 3);
@@ -268,7 +351,7 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
     if (cg.x >= 0) {
       float* d = p.delta + (size_t)i * kOut;
 #pragma unroll
-      for (int o = 0; o < kOut; ++o) d[o] = s * (v[o] + bias[128 + o]);
+      for (int o = 0; o < kOut; ++o) d[o] = s * v[o];
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -371,18 +454,19 @@ struct TrainArgs {
 constexpr int kTrOffDOT = 0;          // 16 x 128 (rows 0..5 used)
 constexpr int kTrOffDZ2T = 4096;      // 64 x 128
 constexpr int kTrOffDZ1T = 20480;     // 64 x 128
-constexpr int kTrOffX = 36864;        // 128 x 64
+constexpr int kTrOffX = 36864;        // 128 x 64 (column 54 = 1)
 constexpr int kTrOffXT = 53248;       // 64 x 128
-constexpr int kTrOffG1 = 69632;
-constexpr int kTrOffG1T = 86016;
-constexpr int kTrOffG2 = 102400;
-constexpr int kTrOffG2T = 118784;
-constexpr int kTrOffDO = 135168;      // 128 x 16
-constexpr int kTrOffDZ2 = 139264;     // 128 x 64
-constexpr int kTrOffW = 155648;       // full image
-constexpr int kTrOffF = kTrOffW + kImgBytes;   // b1|b2|b3 (144), gb (144), loss
+constexpr int kTrOffG1 = 69632;       // 128 x 80 (column 64 = 1)
+constexpr int kTrOffG1T = 90112;      // 64 x 128
+constexpr int kTrOffG2 = 106496;      // 128 x 80 (column 64 = 1)
+constexpr int kTrOffG2T = 126976;     // 64 x 128
+constexpr int kTrOffDO = 143360;      // 128 x 16
+constexpr int kTrOffDZ2 = 147456;     // 128 x 64
+constexpr int kTrOffW = 163840;       // full image
+constexpr int kTrOffF = kTrOffW + kImgBytes;   // gb (144), loss
 constexpr int kTrOffBar = kTrOffF + 1280;
 constexpr int kTrSmem = kTrOffBar + 16;
+static_assert(kTrSmem <= 227 * 1024, "training kernel shared memory");
 // TMEM columns
 constexpr int kTmZ1 = 0, kTmZ2 = 64, kTmO = 128, kTmDG2 = 160, kTmDG1 = 224, kTmDW3 = 288,
               kTmDW2 = 352, kTmDW1 = 416;
@@ -410,8 +494,7 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
   const int n_tiles = p.tiles[f];
   if ((int)blockIdx.x >= n_tiles) return;
   unsigned char* sm = smem;
-  float* bias = reinterpret_cast<float*>(sm + kTrOffF);
-  float* gb = bias + 144;
+  float* gb = reinterpret_cast<float*>(sm + kTrOffF);
   float* lsum = gb + 144;
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTrOffBar);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTrOffBar + 8);
@@ -423,12 +506,10 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
     const uint4* src = reinterpret_cast<const uint4*>(p.wimg + (size_t)f * kImgBytes);
     uint4* dst = reinterpret_cast<uint4*>(sm + kTrOffW);
     for (int k = tid; k < kImgBytes / 16; k += 128) dst[k] = __ldg(src + k);
-    const float* pf = p.params + (size_t)f * kParams;
-    for (int k = tid; k < 144; k += 128) {
-      bias[k] = k < 64 ? pf[kB1 + k] : (k < 128 ? pf[kB2 + k - 64] : pf[kB3 + k - 128]);
-      gb[k] = 0.0f;
-    }
+    for (int k = tid; k < 144; k += 128) gb[k] = 0.0f;
     if (tid == 0) *lsum = 0.0f;
+    init_hidden_tail(sm + kTrOffG1, tid, 128);
+    init_hidden_tail(sm + kTrOffG2, tid, 128);
   }
   if (tid < 32) {
     tc::tmem_alloc(tslot, kTrTmemCols);
@@ -451,6 +532,7 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
   bool ok = true;
   bool first = true;
   float v[64], u[64];
+  uint32_t g[32];
   for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
     const long long j = (long long)t * kTile + tid;
     long long row;
@@ -483,7 +565,10 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
 #pragma unroll
       for (int o = 0; o < kOut; ++o) tg[o] = 0.0f;
     }
-    tc::put_row64(sm + kTrOffX, tid, v);
+    v[kOneX] = 1.0f;
+#pragma unroll
+    for (int k = kOneX + 1; k < 64; ++k) v[k] = 0.0f;
+    put_row_f32(sm + kTrOffX, tid, v, 64);
     tc::put_col(sm + kTrOffXT, tid, v, 64);
     fence_proxy_async();
     tc::fence_before_sync();
@@ -500,42 +585,46 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
     phase ^= 1;
     if (!ok) break;
     tc::fence_after_sync();
-    tc::ld32(lb + kTmZ1, v);
-    tc::ld32(lb + kTmZ1 + 32, v + 32);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) v[k] = gelu(v[k] + bias[k]);
-    tc::put_row64(sm + kTrOffG1, tid, v);
-    tc::put_col(sm + kTrOffG1T, tid, v, 64);
+    for (int hlf = 0; hlf < 2; ++hlf) {
+      tc::ld32(lb + kTmZ1 + 32 * hlf, u);
+#pragma unroll
+      for (int c = 0; c < 16; ++c) g[16 * hlf + c] = gelu2(u[2 * c], u[2 * c + 1]);
+    }
+    put_row_packed(sm + kTrOffG1, tid, g, kKH);
+    put_col_packed(sm + kTrOffG1T, tid, g);
     fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     // forward layer 2
     if (tid == 0) {
       tc::fence_after_sync();
-      for (int kk = 0; kk < 4; ++kk)
-        tc::mma(tm + kTmZ2, tc::img_desc(s0 + kTrOffG1, 64, kk),
-                tc::img_desc(sW + kImgW2, 64, kk), id64, kk);
+      for (int kk = 0; kk < 5; ++kk)
+        tc::mma(tm + kTmZ2, tc::img_desc(s0 + kTrOffG1, kKH, kk),
+                tc::img_desc(sW + kImgW2, kKH, kk), id64, kk);
       tc::commit(bar);
     }
     ok = wait_all(bar, phase, p.wait_ns, p.err, 12);
     phase ^= 1;
     if (!ok) break;
     tc::fence_after_sync();
-    tc::ld32(lb + kTmZ2, v);
-    tc::ld32(lb + kTmZ2 + 32, v + 32);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) v[k] = gelu(v[k] + bias[64 + k]);
-    tc::put_row64(sm + kTrOffG2, tid, v);
-    tc::put_col(sm + kTrOffG2T, tid, v, 64);
+    for (int hlf = 0; hlf < 2; ++hlf) {
+      tc::ld32(lb + kTmZ2 + 32 * hlf, u);
+#pragma unroll
+      for (int c = 0; c < 16; ++c) g[16 * hlf + c] = gelu2(u[2 * c], u[2 * c + 1]);
+    }
+    put_row_packed(sm + kTrOffG2, tid, g, kKH);
+    put_col_packed(sm + kTrOffG2T, tid, g);
     fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     // forward layer 3
     if (tid == 0) {
       tc::fence_after_sync();
-      for (int kk = 0; kk < 4; ++kk)
-        tc::mma(tm + kTmO, tc::img_desc(s0 + kTrOffG2, 64, kk),
-                tc::img_desc(sW + kImgW3, 64, kk), id16, kk);
+      for (int kk = 0; kk < 5; ++kk)
+        tc::mma(tm + kTmO, tc::img_desc(s0 + kTrOffG2, kKH, kk),
+                tc::img_desc(sW + kImgW3, kKH, kk), id16, kk);
       tc::commit(bar);
     }
     ok = wait_all(bar, phase, p.wait_ns, p.err, 13);
@@ -549,7 +638,7 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
       for (int o = 0; o < 16; ++o) d[o] = 0.0f;
 #pragma unroll
       for (int o = 0; o < kOut; ++o) {
-        const float r = v[o] + bias[128 + o] - tg[o];
+        const float r = v[o] - tg[o];
         l = fmaf(w * r, r, l);
         d[o] = 2.0f * scale * w * r;
       }
@@ -594,8 +683,8 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
     tc::ld32(lb + kTmZ2, u);
     tc::ld32(lb + kTmZ2 + 32, u + 32);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) v[k] *= gelu_grad(u[k] + bias[64 + k]);
-    tc::put_row64(sm + kTrOffDZ2, tid, v);
+    for (int k = 0; k < 64; ++k) v[k] *= gelu_grad(u[k]);
+    put_row_f32(sm + kTrOffDZ2, tid, v, 64);
     tc::put_col(sm + kTrOffDZ2T, tid, v, 64);
 #pragma unroll 4
     for (int k = 0; k < 64; ++k) {
@@ -625,7 +714,7 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
     tc::ld32(lb + kTmZ1, u);
     tc::ld32(lb + kTmZ1 + 32, u + 32);
 #pragma unroll
-    for (int k = 0; k < 64; ++k) v[k] *= gelu_grad(u[k] + bias[k]);
+    for (int k = 0; k < 64; ++k) v[k] *= gelu_grad(u[k]);
     tc::put_col(sm + kTrOffDZ1T, tid, v, 64);
 #pragma unroll 4
     for (int k = 0; k < 64; ++k) {
@@ -651,22 +740,22 @@ __global__ void __launch_bounds__(128, 1) k_band_train(const __grid_constant__ T
   __syncthreads();
   if (ok) {
     tc::fence_after_sync();
-    float* g = p.grad + (size_t)f * kParams;
+    float* gr = p.grad + (size_t)f * kParams;
     if (tid < 64) {  // warps 0 and 1 hold rows 0..63 of the weight gradients
       tc::ld32(lb + kTmDW1, v);
       tc::ld32(lb + kTmDW1 + 32, v + 32);
       tc::ld32(lb + kTmDW2, u);
       tc::ld32(lb + kTmDW2 + 32, u + 32);
-      for (int k = 0; k < kIn; ++k) atomicAdd(&g[kW1 + tid * kInP + k], v[k]);
-      for (int k = 0; k < 64; ++k) atomicAdd(&g[kW2 + tid * kHid + k], u[k]);
+      for (int k = 0; k < kIn; ++k) atomicAdd(&gr[kW1 + tid * kInP + k], v[k]);
+      for (int k = 0; k < 64; ++k) atomicAdd(&gr[kW2 + tid * kHid + k], u[k]);
       tc::ld32(lb + kTmDW3, v);
       tc::ld32(lb + kTmDW3 + 32, v + 32);
       if (tid < kOut)
-        for (int k = 0; k < 64; ++k) atomicAdd(&g[kW3 + tid * kHid + k], v[k]);
+        for (int k = 0; k < 64; ++k) atomicAdd(&gr[kW3 + tid * kHid + k], v[k]);
     }
     for (int k = tid; k < 144; k += 128) {
       const int dst = k < 64 ? kB1 + k : (k < 128 ? kB2 + k - 64 : kB3 + k - 128);
-      if (k < 128 || k - 128 < kOut) atomicAdd(&g[dst], gb[k]);
+      if (k < 128 || k - 128 < kOut) atomicAdd(&gr[dst], gb[k]);
     }
     if (tid == 0) atomicAdd(&p.loss[f], *lsum);
   } else {
@@ -709,22 +798,22 @@ __global__ void k_band_pack(const float* params, unsigned char* wimg) {
   const float* pf = params + (size_t)f * kParams;
   const int byte = e * 2;
   int r, k;
-  float val;
+  float val = 0.0f;
   if (byte < kImgW2) {
-    img_rc(byte - kImgW1, 64, r, k);
-    val = pf[kW1 + r * kInP + k];
+    img_rc(byte - kImgW1, 64, r, k);  // W1 | b1 at column 54
+    val = k < kIn ? pf[kW1 + r * kInP + k] : (k == kOneX ? pf[kB1 + r] : 0.0f);
   } else if (byte < kImgW3) {
-    img_rc(byte - kImgW2, 64, r, k);
-    val = pf[kW2 + r * kHid + k];
+    img_rc(byte - kImgW2, kKH, r, k);  // W2 | b2 at column 64
+    val = k < kHid ? pf[kW2 + r * kHid + k] : (k == kHid ? pf[kB2 + r] : 0.0f);
   } else if (byte < kImgW2T) {
-    img_rc(byte - kImgW3, 64, r, k);
-    val = pf[kW3 + r * kHid + k];
+    img_rc(byte - kImgW3, kKH, r, k);  // W3 | b3 at column 64
+    if (r < kOut) val = k < kHid ? pf[kW3 + r * kHid + k] : (k == kHid ? pf[kB3 + r] : 0.0f);
   } else if (byte < kImgW3T) {
     img_rc(byte - kImgW2T, 64, r, k);  // r = input unit, k = output unit
     val = pf[kW2 + k * kHid + r];
   } else {
     img_rc(byte - kImgW3T, 16, r, k);  // r = hidden unit, k = output
-    val = pf[kW3 + k * kHid + r];
+    if (k < kOut) val = pf[kW3 + k * kHid + r];
   }
   *reinterpret_cast<__nv_bfloat16*>(wimg + (size_t)f * kImgBytes + byte) =
       __float2bfloat16_rn(val);

@@ -197,10 +197,23 @@ class BandCase:
     eps: np.ndarray | None = None
     sources: list = field(default_factory=list)
 
+    def extra_z(self, pad: int) -> int:
+        """Vacuum cells added at the high-z end of a grid with `pad` cells per
+        side so that nz is a multiple of 4 (16-byte rows: vector loads of the
+        z-face band stencil, and the TMA stencil path)."""
+        return (-(int(self.size[2]) + 2 * pad)) % 4
+
     def grid(self, pad: int, boundary: str, pml_layers: int = 0, resolution: float = 1.0,
-             path: str = "generic", cpml: CPMLSpec | None = None) -> EMGrid3D:
-        """This case embedded with `pad` vacuum cells on every side."""
-        n = tuple(int(v) + 2 * pad for v in self.size)
+             path: str = "generic", cpml: CPMLSpec | None = None,
+             extra_z: int | None = None) -> EMGrid3D:
+        """This case embedded with `pad` vacuum cells on every side and
+        `extra_z` (default: ``self.extra_z(pad)``) more vacuum cells at the
+        high-z end; the interior starts at (pad, pad, pad) and any
+        `pml_layers` of the boundary are the outermost cells."""
+        ez = self.extra_z(pad) if extra_z is None else int(extra_z)
+        n = [int(v) + 2 * pad for v in self.size]
+        n[2] += ez
+        n = tuple(n)
         g = EMGrid3D(n, resolution=resolution, boundary=boundary, pml_layers=pml_layers,
                      cpml=cpml, path=path)
         if self.eps is not None:
@@ -251,23 +264,48 @@ def _copy_box(dst: EMGrid3D, src: EMGrid3D, off) -> None:
         dst.set_field(name, src.field(name)[ox:ox + nx, oy:oy + ny, oz:oz + nz].contiguous())
 
 
+def _perturb_band(g: EMGrid3D, rel: float, gen) -> None:
+    """Add Gaussian noise of `rel` times the band's RMS field to the band layers."""
+    import torch
+
+    nx, ny, nz = g.size
+    L = BAND_LAYERS
+    mask = torch.ones((nx, ny, nz), dtype=torch.bool, device=f"cuda:{g._h_key[1]}")
+    mask[L:nx - L, L:ny - L, L:nz - L] = False
+    for name in COMPONENTS:
+        f = g.field(name)
+        rms = torch.sqrt(torch.mean(f[mask] ** 2))
+        noise = torch.randn(f.shape, device=f.device, generator=gen) * (rel * rms)
+        g.set_field(name, torch.where(mask, f + noise, f))
+
+
 def collect_traces(model: LearnedBand, case: BandCase, n_steps: int, every: int = 2,
-                   start: int = 0, ref_pml: int = 16, resolution: float = 1.0) -> None:
+                   start: int = 0, ref_pml: int = 16, resolution: float = 1.0,
+                   noise: float = 0.0, seed: int = 0) -> None:
     """Training rows for `case` (band grid = interior + 3 vacuum layers per side).
 
     The padded reference grid adds `ref_pml` CPML layers around the band grid.
     Every `every` steps from `start`, the band grid is loaded with the
     reference state, takes one plain (PEC) step, and its outer cells are
-    compared with the reference one step later.
+    compared with the reference one step later.  With `noise` > 0 the band
+    layers of the loaded state are perturbed by Gaussian noise of that size
+    relative to their RMS (the target stays the unperturbed reference), which
+    teaches the networks to pull a perturbed band back.
     """
-    ref = case.grid(BAND_LAYERS + ref_pml, "cpml", ref_pml, resolution, path="auto")
-    trunc = BandCase(case.size, case.eps, []).grid(BAND_LAYERS, "pec", 0, resolution)
+    import torch
+
+    ez = case.extra_z(BAND_LAYERS)
+    ref = case.grid(BAND_LAYERS + ref_pml, "cpml", ref_pml, resolution, path="auto", extra_z=ez)
+    trunc = BandCase(case.size, case.eps, []).grid(BAND_LAYERS, "pec", 0, resolution, extra_z=ez)
     ref.prepare()
     trunc.prepare(ref._dt)
     off = (ref_pml, ref_pml, ref_pml)
+    gen = torch.Generator(device=f"cuda:{ref._h_key[1]}").manual_seed(int(seed))
     for n in range(int(n_steps)):
         if n >= start and (n - start) % every == 0:
             _copy_box(trunc, ref, off)
+            if noise > 0.0:
+                _perturb_band(trunc, noise, gen)
             trunc.step(1)
             ref.step(1)
             model.collect(trunc, ref, off)

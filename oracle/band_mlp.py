@@ -8,9 +8,9 @@ compute:
 * face ownership of the outer cell layer and the per-face cell lists,
 * the 54-value stencil features (Ex..Hz with H scaled by eta0 over the 3
   outermost layers x 3 tangential offsets) and their RMS normalisation,
-* the per-face network 54 -> 64 -> 64 -> 6 with tanh-form GELU, BF16
-  weights/activations and wide accumulation (``emulate=True``) or exact
-  FP64 arithmetic (``emulate=False``),
+* the per-face network 54 -> 64 -> 64 -> 6 with tanh-form GELU: BF16
+  weights, biases and activations, packed-BF16 GELU arithmetic and wide
+  accumulation (``emulate=True``) or exact FP64 arithmetic (``emulate=False``),
 * the weighted-MSE loss and its parameter gradients,
 * the band correction applied after a plain Yee step.
 
@@ -84,11 +84,28 @@ def gelu_grad(x):
     return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * GELU_C0 * (1.0 + 3.0 * GELU_C1 * x * x)
 
 
+def gelu_bf16(z):
+    """The kernels' packed-BF16 GELU: x = bf16(z); p = bf16(x^2 * c01 + c0) with
+    x^2 rounded first; u = bf16(x p); t = bf16(tanh u); h = x / 2;
+    g = bf16(h t + h) (tanh exact here, tanh.approx.bf16x2 on the GPU)."""
+    r = lambda a: bf16(a).astype(np.float64)
+    c0 = float(bf16(np.float32(GELU_C0)).reshape(-1)[0])
+    c01 = float(bf16(np.float32(GELU_C0 * GELU_C1)).reshape(-1)[0])
+    x = r(z)
+    p = r(r(x * x) * c01 + c0)
+    u = r(x * p)
+    t = r(np.tanh(u))
+    h = x * 0.5
+    return r(h * t + h)
+
+
 def _weights(p, emulate):
+    """Weights (BF16 when emulating) and biases (BF16 when emulating: the
+    kernels carry them as a BF16 column of the weight image)."""
     w1, b1, w2, b2, w3, b3 = unpack(np.asarray(p, dtype=np.float32 if emulate else np.float64))
     q = bf16 if emulate else (lambda a: np.asarray(a, dtype=np.float64))
-    return (q(w1).astype(np.float64), b1.astype(np.float64), q(w2).astype(np.float64),
-            b2.astype(np.float64), q(w3).astype(np.float64), b3.astype(np.float64))
+    return (q(w1).astype(np.float64), q(b1).astype(np.float64), q(w2).astype(np.float64),
+            q(b2).astype(np.float64), q(w3).astype(np.float64), q(b3).astype(np.float64))
 
 
 def forward(p: np.ndarray, x: np.ndarray, emulate: bool = True):
@@ -99,14 +116,11 @@ def forward(p: np.ndarray, x: np.ndarray, emulate: bool = True):
     if emulate:
         X = bf16(X).astype(np.float64)
     w1, b1, w2, b2, w3, b3 = _weights(p, emulate)
+    act = gelu_bf16 if emulate else gelu
     z1 = X @ w1.T + b1
-    g1 = gelu(z1)
-    if emulate:
-        g1 = bf16(g1).astype(np.float64)
+    g1 = act(z1)
     z2 = g1 @ w2.T + b2
-    g2 = gelu(z2)
-    if emulate:
-        g2 = bf16(g2).astype(np.float64)
+    g2 = act(z2)
     o = g2 @ w3.T + b3
     return o[:, :N_OUT]
 
@@ -120,10 +134,11 @@ def loss_and_grad(p: np.ndarray, x: np.ndarray, tgt: np.ndarray, w: np.ndarray, 
     q = (lambda a: bf16(a).astype(np.float64)) if emulate else (lambda a: a)
     X = q(X)
     w1, b1, w2, b2, w3, b3 = _weights(p, emulate)
+    act = gelu_bf16 if emulate else gelu
     z1 = X @ w1.T + b1
-    g1 = q(gelu(z1))
+    g1 = act(z1)
     z2 = g1 @ w2.T + b2
-    g2 = q(gelu(z2))
+    g2 = act(z2)
     o = (g2 @ w3.T + b3)[:, :N_OUT]
     r = o - tgt
     ww = np.asarray(w, dtype=np.float64)[:, None]
