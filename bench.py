@@ -1,7 +1,7 @@
 """Throughput benchmark of the 3D FDTD hot path (Gcell-updates/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c1|c3]
+                    [--workload c2|c1|c3|c5]
 
 A bench step is one complete simulation of the workload: zero the fields,
 run all its leapfrog steps with probe recording.  Default workload (c2):
@@ -49,7 +49,10 @@ WORKLOADS = {
     "c2": (128, 1000, 10, "fdtd3d-128^3-cpml10-sphere-eps4-pulse-16probes"),
     "c1": (64, 500, 8, "fdtd3d-64^3-cpml8-vacuum-pulse-8probes"),
     "c3": (512, 200, 12, "fdtd3d-512^3-cpml12-smoothnoise-eps1to12"),
+    # batched learned boundary: 64 grids, interior sides uniform in [48, 160]
+    "c5": (64, 1000, 3, "batch64-sides48to160-eps1to6-dipoles-learnedband3-vs-cpml10"),
 }
+BAND_WEIGHTS = ROOT / "jaxphys_b200" / "em" / "band_weights.npz"
 
 # DRAM bytes per leapfrog step (CPML shell launch + interior launch) from the
 # ncu capture of the same workload and launch shape
@@ -323,6 +326,148 @@ def run_ours(args, world, rank, local, pg):
         print(json.dumps(line), flush=True)
 
 
+def c5_cases(seed: int = 5, n_grids: int = 64):
+    """The batched learned-boundary workload: seeded interior sides uniform in
+    [48, 160] (half cubes, half boxes), smoothed eps_r in [1, 6], one dipole of
+    random position and orientation per grid (Gaussian-modulated sinusoid,
+    f0 = 0.05/dt, width 30 steps)."""
+    from jaxphys_b200.em.learned import random_case
+
+    rng = np.random.default_rng(seed)
+    cases = []
+    for _ in range(n_grids):
+        if rng.random() < 0.5:
+            s = int(rng.integers(48, 161))
+            size = (s, s, s)
+        else:
+            size = tuple(int(v) for v in rng.integers(48, 161, 3))
+        cases.append(random_case(rng, size, eps_range=(1.0, 6.0), n_sources=1, margin=4))
+    return cases
+
+
+def run_batch(args, world, rank, local, pg):
+    """c5: the same 64-grid batch with the learned 3-cell band, with 10-cell
+    CPML, with the CPML of equal measured error (4 cells) and with bare PEC
+    walls.  value = interior cell updates per second of the learned run."""
+    import torch
+
+    from jaxphys_b200.em.batch import FDTDBatch
+    from jaxphys_b200.em.learned import BAND_LAYERS, LearnedBand, reflection_db, train_band
+
+    torch.cuda.set_device(local)
+    n_grids, nsteps, _, wname = WORKLOADS["c5"]
+    cases = c5_cases(seed=5 + rank, n_grids=n_grids)
+    interior = sum(int(np.prod(c.size)) for c in cases)
+    model = LearnedBand.load(BAND_WEIGHTS) if BAND_WEIGHTS.exists() else train_band(seed=0)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    def build(kind):
+        grids = []
+        for c in cases:
+            if kind in ("learned", "pec"):
+                g = c.grid(BAND_LAYERS, "pec", 0)
+            else:
+                k = int(kind[4:])
+                g = c.grid(k, "cpml", k)
+            g.prepare()
+            grids.append(g)
+        b = FDTDBatch(grids)
+        if kind == "learned":
+            b.set_band(model)
+        return grids, b
+
+    results = {}
+    launches = 0
+    sampler = None
+    for kind in ("learned", "cpml10", "cpml4", "pec"):
+        grids, b = build(kind)
+        cells = sum(int(np.prod(g.size)) for g in grids)
+        for _ in range(max(args.warmup, 1)):
+            b.reset()
+            b.run(nsteps)
+        barrier()
+        if kind == "learned":
+            sampler = ClockSampler(local)
+            sampler.start()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        for k in range(args.steps):
+            b.reset()
+            ev[k][0].record(stream)
+            b.run(nsteps)
+            ev[k][1].record(stream)
+        barrier()
+        clocks = sampler.stop() if kind == "learned" else None
+        ms = float(sum(a.elapsed_time(bb) for a, bb in ev))
+        if pg is not None:
+            t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        for g in grids[:2]:
+            g.check()
+        results[kind] = {"ms_per_step": round(ms / args.steps, 3), "grid_cells": cells,
+                         "interior_gcell_s": round(interior * nsteps * args.steps * world / ms / 1e6, 3),
+                         "grid_gcell_s": round(cells * nsteps * args.steps * world / ms / 1e6, 3)}
+        if kind == "learned":
+            results[kind]["clocks"] = clocks
+            # per leapfrog step: batched H, E, sources, band inference, band apply
+            launches = 5 * nsteps * args.steps
+        b.close()
+        for g in grids:
+            g._release()
+    model.check()
+    refl = {}
+    if rank == 0 and args.reflection > 0:
+        small = sorted(range(len(cases)), key=lambda i: np.prod(cases[i].size))[:args.reflection]
+        for i in small:
+            r = reflection_db(cases[i], nsteps, model=model, cpml_layers=(4, 10), every=10)
+            refl[str(cases[i].size)] = {k: round(v, 2) for k, v in r.items()}
+    lr = results["learned"]
+    peak, peak_kind = measured_peaks()
+    # algorithmic bytes of one leapfrog step of the learned batch: the Yee
+    # update (6 components read + written, eps read: 52 B per cell) and the
+    # band (outer cells: 24 B stencil centre read, 24 B correction written
+    # and read back, 24 B field read-modify-write: 120 B per outer cell)
+    outer = sum(int(np.prod(np.array(c.size) + 6)) - int(np.prod(np.array(c.size) + 4))
+                for c in cases)
+    step_bytes = lr["grid_cells"] * 52.0 + outer * 120.0
+    achieved = step_bytes / (lr["ms_per_step"] / nsteps * 1e-3) / 1e9
+    line = {
+        "metric": "learned-band batch interior Gcell-updates/s",
+        "value": lr["interior_gcell_s"],
+        "unit": "Gcell/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": lr["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 fields, bf16 MLP with f32 accumulation",
+        "data": "synthetic (seeded sizes, eps_r maps, dipoles)",
+        "config": {"workload": wname, "grids": n_grids, "interior_cells": interior,
+                   "leapfrog_steps_per_step": nsteps, "band_layers": BAND_LAYERS,
+                   "l2": "inputs larger than L2 (>= 360 MB of fields)",
+                   "parallelism": f"independent batch per GPU x{world}"},
+        "compare": {k: results[k] for k in ("cpml10", "cpml4", "pec")},
+        "speedup_vs_cpml10": round(results["cpml10"]["ms_per_step"] / lr["ms_per_step"], 3),
+        "speedup_vs_cpml4_equal_error": round(results["cpml4"]["ms_per_step"] / lr["ms_per_step"], 3),
+        "reflection_db": refl,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                     "kernel": "whole learned-batch leapfrog step (Yee + band)"},
+        "gpu_launches": launches,
+        "clocks": lr.pop("clocks"),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def cpu_baseline(workload: str, budget_s: float = 10.0, steps: int | None = None):
     """The FP64 C restatement of the reference step on every host thread, on a
     bounded sample (a prefix of the workload's leapfrog steps)."""
@@ -356,6 +501,11 @@ def cpu_baseline(workload: str, budget_s: float = 10.0, steps: int | None = None
 
 def run_reference(args, world, rank):
     if rank != 0:
+        return
+    if args.workload == "c5":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has neither a "
+                          "learned boundary nor batched grids; its CPU Yee path is timed under "
+                          "the c1/c2/c3 workloads"}), flush=True)
         return
     n, nsteps, pml, wname = WORKLOADS[args.workload]
     # each bench step: a bounded sample of the workload on the host cores
@@ -402,11 +552,15 @@ def main():
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="c2")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reflection", type=int, default=2,
+                    help="c5: grids whose reflection is measured against a padded reference")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "c5":
+            run_batch(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:

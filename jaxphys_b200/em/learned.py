@@ -317,6 +317,71 @@ def collect_traces(model: LearnedBand, case: BandCase, n_steps: int, every: int 
     trunc._release()
 
 
+def collect_onpolicy(model: LearnedBand, case: BandCase, n_steps: int, every: int = 2,
+                     resync: int = 80, ref_pml: int = 16, resolution: float = 1.0) -> dict:
+    """Training rows from the band's own trajectory (DAgger).
+
+    The band grid runs with `model` in the loop next to the padded CPML
+    reference.  Every `every` steps its state X is labelled with the exact
+    one-step response given X: a copy of the reference in which the band
+    grid's box is replaced by X takes one step, and the outer cells of the
+    band grid's plain step from X are compared with it.  Every `resync` steps
+    the band grid is reset to the reference state, so the visited states stay
+    near the reference trajectory.  Returns {"max_rel": largest ratio of the
+    band grid's field norm to the reference's} as a stability indicator.
+    """
+    import torch
+
+    from .batch import FDTDBatch
+
+    ez = case.extra_z(BAND_LAYERS)
+    pad = BAND_LAYERS + ref_pml
+    ref = case.grid(pad, "cpml", ref_pml, resolution, path="auto", extra_z=ez)
+    hyb = case.grid(pad, "cpml", ref_pml, resolution, path="generic", extra_z=ez)
+    live = case.grid(BAND_LAYERS, "pec", 0, resolution, extra_z=ez)
+    plain = BandCase(case.size, case.eps, []).grid(BAND_LAYERS, "pec", 0, resolution, extra_z=ez)
+    ref.prepare()
+    dt = ref._dt
+    for g in (hyb, live, plain):
+        g.prepare(dt)
+    b = FDTDBatch([live])
+    b.set_band(model)
+    off = (ref_pml, ref_pml, ref_pml)
+    nx, ny, nz = live.size
+    box = (slice(off[0], off[0] + nx), slice(off[1], off[1] + ny), slice(off[2], off[2] + nz))
+    max_rel = 0.0
+    for n in range(int(n_steps)):
+        if n % resync == 0:
+            for name in COMPONENTS:
+                live.set_field(name, ref.field(name)[box].contiguous())
+        if n % every == 0 and n % resync != 0:
+            cur = {name: live.field(name) for name in COMPONENTS}
+            for name in COMPONENTS:
+                full = ref.field(name)
+                full[box] = cur[name]
+                hyb.set_field(name, full)
+                plain.set_field(name, cur[name])
+            hyb.step(1)
+            plain.step(1)
+            model.collect(plain, hyb, off)
+        ref.step(1)
+        b.run(1, use_graph=False)
+        if n % 20 == 19:
+            e_live = float(torch.linalg.vector_norm(live.field("ez")))
+            e_ref = float(torch.linalg.vector_norm(ref.field("ez")[box])) + 1e-30
+            if not math.isfinite(e_live):
+                max_rel = float("inf")
+                for name in COMPONENTS:
+                    live.set_field(name, ref.field(name)[box].contiguous())
+            else:
+                max_rel = max(max_rel, e_live / e_ref)
+    b.close()
+    for g in (ref, hyb, live, plain):
+        g._release()
+    model.check()
+    return {"max_rel": max_rel}
+
+
 def reflection_db(case: BandCase, n_steps: int, model: LearnedBand | None = None,
                   cpml_layers: tuple = (10,), ref_pml: int = 16, every: int = 10,
                   resolution: float = 1.0, pec: bool = True) -> dict:
@@ -387,3 +452,56 @@ def reflection_db(case: BandCase, n_steps: int, model: LearnedBand | None = None
     if model is not None:
         model.check()
     return out
+
+
+def train_band(seed: int = 0, n_cases: int = 8, size_range=(18, 40), n_steps: int = 320,
+               noise=(0.03,), schedule=((2e-3, 2000), (1e-3, 2000), (3e-4, 2000),
+                                            (1e-4, 1000)),
+               dagger_rounds: int = 2, dagger_steps: int = 400,
+               dagger_schedule=((3e-4, 1500), (1e-4, 1000)),
+               batch_rows: int = 8192, freq_range=(0.035, 0.07), width_range=(20.0, 40.0),
+               eps_range=(1.0, 6.0), device: int | None = None, log=None) -> LearnedBand:
+    """Train a band from scratch on the GPU (the recipe of the shipped weights).
+
+    `n_cases` random boxes (sides in `size_range`, smoothed permittivity in
+    `eps_range`, 1-2 dipoles of random position / orientation driven by
+    Gaussian-modulated sinusoids of centre frequency in `freq_range` / dt and
+    width in `width_range` steps); for each, one trace pass per entry of
+    `noise` (band-state perturbation level); Adam with the piecewise constant
+    learning-rate `schedule` of (lr, iterations); then `dagger_rounds` rounds
+    of on-policy rows (``collect_onpolicy``, `dagger_steps` steps per case)
+    each followed by `dagger_schedule`.
+    """
+    rng = np.random.default_rng(seed)
+    model = LearnedBand(seed=seed, device=device)
+    cases = []
+    for i in range(int(n_cases)):
+        size = tuple(int(v) for v in rng.integers(size_range[0], size_range[1] + 1, 3))
+        case = random_case(rng, size, eps_range=eps_range, n_sources=int(rng.integers(1, 3)),
+                           dt_freq=float(rng.uniform(*freq_range)),
+                           width=float(rng.uniform(*width_range)))
+        cases.append(case)
+        for k, lvl in enumerate(noise):
+            collect_traces(model, case, n_steps=n_steps, every=2, start=k % 2, noise=float(lvl),
+                           seed=seed * 1000 + i * 10 + k)
+    it = 0
+
+    def fit(sched, tag):
+        nonlocal it
+        for lr, n in sched:
+            h = model.train(int(n), batch_rows=batch_rows, lr=float(lr), seed=seed * 7919 + it)
+            it += 1
+            if log is not None:
+                log(f"{tag} lr {lr:g}: mean loss of the last 100 steps {float(np.mean(h[-100:])):.4g}")
+
+    fit(schedule, "traces")
+    for r in range(int(dagger_rounds)):
+        worst = 0.0
+        for case in cases:
+            st = collect_onpolicy(model, case, n_steps=dagger_steps)
+            worst = max(worst, st["max_rel"])
+        if log is not None:
+            log(f"on-policy round {r}: rows {int(model.dataset_size().sum())}, "
+                f"largest field-norm ratio to the reference {worst:.3g}")
+        fit(dagger_schedule, f"round {r}")
+    return model

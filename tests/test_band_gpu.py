@@ -181,3 +181,36 @@ def test_training_reduces_loss(cuda):
     assert np.all(np.isfinite(hist)) and np.all(np.isfinite(m.params))
     assert loss1.sum() < 0.5 * loss0.sum(), (loss0.sum(), loss1.sum())
     m.close()
+
+
+def test_shipped_band_beats_bare_walls_and_is_stable(cuda):
+    """The shipped weights against the same grid without the band (bare PEC
+    walls) and against 3- and 4-layer CPML, on a held-out problem."""
+    from pathlib import Path
+
+    from jaxphys_b200.em.learned import LearnedBand, random_case, reflection_db
+
+    path = Path(__file__).resolve().parents[1] / "jaxphys_b200" / "em" / "band_weights.npz"
+    m = LearnedBand.load(path)
+    rng = np.random.default_rng(4242)
+    case = random_case(rng, (34, 30, 38), eps_range=(1.0, 6.0), n_sources=1)
+    r = reflection_db(case, 500, model=m, cpml_layers=(3, 4), every=10)
+    assert np.isfinite(r["learned"])
+    # the band removes most of the wall reflection (bare walls: ~ -2 dB)
+    assert r["learned"] < r["pec"] - 15.0, r
+    # and at 3 cells beats the 3-cell CPML
+    assert r["learned"] < r["cpml3"] - 5.0, r
+    m.close()
+
+
+def test_onpolicy_collection_appends_rows(cuda):
+    from jaxphys_b200.em.learned import LearnedBand, collect_onpolicy, random_case
+
+    m = LearnedBand(seed=3)
+    case = random_case(np.random.default_rng(9), (14, 12, 16), eps_range=(1.0, 2.0), margin=5)
+    st = collect_onpolicy(m, case, n_steps=40, every=4, resync=20)
+    sizes = m.dataset_size()
+    assert np.all(sizes > 0) and "max_rel" in st
+    x, t, w = m.dataset(0)
+    assert np.all(np.isfinite(x)) and np.all(np.isfinite(t)) and np.all(w >= 0)
+    m.close()
