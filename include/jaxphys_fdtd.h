@@ -204,8 +204,11 @@ int jxf_batch3d_probes(jxf_batch3d* b, int32_t grid, int32_t n_steps, float* dst
  *   jxf_band_train     iters Adam steps on batch_rows random rows per face;
  *                      loss[i] (nullable) = summed face losses of step i.
  *   jxf_band_eval      outputs for given normalised feature rows (testing).
- *   jxf_batch3d_set_band attaches a band to a batch of PEC grids (NULL
- *                      detaches); every later step applies it. */
+ *   jxf_batch3d_set_band / jxf_grid3d_set_band attach a band to a batch of
+ *                      PEC grids / to one PEC grid on the generic path (NULL
+ *                      detaches); every later step applies it.  Detach or
+ *                      destroy those grids and batches before destroying
+ *                      the band. */
 #define JXF_BAND_PARAMS 9360
 #define JXF_BAND_FACES 6
 #define JXF_BAND_FEATURES 54
@@ -227,6 +230,7 @@ int jxf_band_train(jxf_band* m, int32_t iters, int32_t batch_rows, float lr, uin
                    float* loss, void* stream);
 int jxf_band_check_error(jxf_band* m, void* stream);
 int jxf_batch3d_set_band(jxf_batch3d* b, jxf_band* m);
+int jxf_grid3d_set_band(jxf_grid3d* g, jxf_band* m);
 
 /* Zero fields and psi, reset the step counter. */
 int jxf_grid3d_reset(jxf_grid3d* g, void* stream);

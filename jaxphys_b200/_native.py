@@ -134,6 +134,7 @@ SIGNATURES = {
     "jxf_band_train": (C.c_int, [_vp, _i32, _i32, C.c_float, C.c_uint64, _vp, _vp]),
     "jxf_band_check_error": (C.c_int, [_vp, _vp]),
     "jxf_batch3d_set_band": (C.c_int, [_vp, _vp]),
+    "jxf_grid3d_set_band": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_run_noalloc": (C.c_int, [C.POINTER(NoAllocDesc), C.POINTER(_vp), _vp, _i32, _vp]),
     "jxf_grid2d_create": (C.c_int, [C.POINTER(Grid2DDesc), C.POINTER(_vp)]),
     "jxf_grid2d_destroy": (C.c_int, [_vp]),

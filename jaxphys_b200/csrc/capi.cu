@@ -241,8 +241,27 @@ std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
 // 3D handle
 // ---------------------------------------------------------------------------
 
+// Device tables of a learned band attached to one grid or a batch: the grids'
+// field pointers, the outer cells in single-face 128-cell tiles, the face of
+// each tile and the correction buffer.
+struct BandTables {
+  jxf_band* band = nullptr;
+  band::GridRef* d_grids = nullptr;
+  int2* d_cells = nullptr;
+  int* d_tile_face = nullptr;
+  float* d_delta = nullptr;
+  int tiles = 0;
+  int ctas = 0;
+};
+
+namespace {
+int band_launch(const BandTables& t, cudaStream_t st);
+void band_release(BandTables& t);
+}  // namespace
+
 struct jxf_grid3d {
   jxf_grid3d_desc d{};
+  BandTables band;          // learned band (PEC, generic path), applied after each step
   int mode = MODE_ABSORB;   // kernel mode: ABSORB (also PEC with unit tables), PERIODIC, CPML
   // x-slab of a decomposed grid: local plane x is global plane x + gx0 of a
   // grid with gnx planes; planes [x_lo, x_hi) are owned, the two outer
@@ -835,6 +854,7 @@ int jxf_grid3d_destroy(jxf_grid3d* g) {
       for (int k = 0; k < TAB_COUNT; ++k) dfree(g->tab[ax][k]);
   for (int ax = 0; ax < 3; ++ax) dfree(g->damp[ax]);
   dfree(g->cb);
+  band_release(g->band);
   dfree(g->d_cells);
   dfree(g->d_terms);
   dfree(g->d_entries);
@@ -1055,6 +1075,7 @@ int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stre
             g->wave_len, g->step);
         CUDA_TRY(cudaGetLastError());
       }
+      if (g->band.band) TRY(band_launch(g->band, st));
       if (probe_out && np > 0) TRY(gather_probes(g, 0, probe_out + (size_t)k * np, st));
       g->step++;
     }
@@ -1512,20 +1533,8 @@ struct jxf_batch3d {
   long long graph_step0 = -1;
   int graph_n = -1;
   size_t cap[7] = {0, 0, 0, 0, 0, 0, 0};  // element capacity of the uploaded tables
-  // learned absorbing band (PEC batches only)
-  jxf_band* band = nullptr;
-  band::GridRef* d_band_grids = nullptr;
-  int2* d_band_cells = nullptr;
-  int* d_band_tile_face = nullptr;
-  float* d_band_delta = nullptr;
-  int band_tiles = 0;
-  int band_ctas = 0;
+  BandTables band;  // learned absorbing band (PEC batches only)
 };
-
-namespace {
-int band_launch(jxf_band* m, const band::GridRef* grids, const int2* cells, const int* tile_face,
-                int n_tiles, int ctas, float* delta, cudaStream_t st);
-}
 
 namespace {
 
@@ -1617,9 +1626,7 @@ int batch_launch_step(jxf_batch3d* b, long long step, float* probe_row, cudaStre
   if (b->n_src_entries > 0)
     k3d_batch_sources<<<(b->n_src_entries + 127) / 128, 128, 0, st>>>(b->d_srcg, b->d_src_entries,
                                                                       b->n_src_entries, step);
-  if (b->band && b->band_tiles > 0)
-    TRY(band_launch(b->band, b->d_band_grids, b->d_band_cells, b->d_band_tile_face,
-                    b->band_tiles, b->band_ctas, b->d_band_delta, st));
+  if (b->band.band) TRY(band_launch(b->band, st));
   if (probe_row && b->n_probes > 0)
     k3d_batch_probes<<<(b->n_probes + 127) / 128, 128, 0, st>>>(b->d_params, b->d_probes,
                                                                 b->n_probes, probe_row);
@@ -1672,10 +1679,7 @@ extern "C" int jxf_batch3d_destroy(jxf_batch3d* b) {
   dfree(b->d_src_entries);
   dfree(b->d_probes);
   dfree(b->d_probe_buf);
-  dfree(b->d_band_grids);
-  dfree(b->d_band_cells);
-  dfree(b->d_band_tile_face);
-  dfree(b->d_band_delta);
+  band_release(b->band);
   delete b;
   return JXF_OK;
 }
@@ -1849,23 +1853,32 @@ int band_check_dims(int nx, int ny, int nz) {
   return JXF_OK;
 }
 
-int band_launch(jxf_band* m, const band::GridRef* grids, const int2* cells, const int* tile_face,
-                int n_tiles, int ctas, float* delta, cudaStream_t st) {
+int band_launch(const BandTables& t, cudaStream_t st) {
+  if (t.tiles <= 0) return JXF_OK;
   band::InferArgs a{};
-  a.grids = grids;
-  a.cells = cells;
-  a.tile_face = tile_face;
-  a.n_tiles = n_tiles;
-  a.wimg = m->d_wimg;
-  a.params = m->d_params;
-  a.delta = delta;
-  a.err = m->d_err;
+  a.grids = t.d_grids;
+  a.cells = t.d_cells;
+  a.tile_face = t.d_tile_face;
+  a.n_tiles = t.tiles;
+  a.wimg = t.band->d_wimg;
+  a.params = t.band->d_params;
+  a.delta = t.d_delta;
+  a.err = t.band->d_err;
   a.wait_ns = wait_limit_ns();
-  band::k_band_infer<band::SRC_GRIDS><<<ctas, 128, band::kInfSmem, st>>>(a);
-  const int n = n_tiles * band::kTile;
-  band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(grids, cells, n, delta);
+  band::k_band_infer<band::SRC_GRIDS><<<t.ctas, 128, band::kInfSmem, st>>>(a);
+  const int n = t.tiles * band::kTile;
+  band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(t.d_grids, t.d_cells, n, t.d_delta);
   CUDA_TRY(cudaGetLastError());
   return JXF_OK;
+}
+
+void band_release(BandTables& t) {
+  dfree(t.d_grids);
+  dfree(t.d_cells);
+  dfree(t.d_tile_face);
+  dfree(t.d_delta);
+  t.band = nullptr;
+  t.tiles = 0;
 }
 
 // CTAs of the inference kernel: resident CTAs per SM (limited by shared
@@ -1963,6 +1976,47 @@ int band_train_pass(jxf_band* m, const band::TrainArgs& a, cudaStream_t st) {
   const int gx = std::max(1, std::min(maxt, std::max(1, sms / 6)));
   band::k_band_train<<<dim3(gx, 6), 128, band::kTrSmem, st>>>(a);
   CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+// Tables for the outer cells of `grids` (PEC, sides >= 8).
+int band_attach(const std::vector<jxf_grid3d*>& grids, jxf_band* m, int device, int64_t* tally,
+                BandTables& t) {
+  if (m->device != device) return fail(JXF_ERR_INVALID, "band and grids on different devices");
+  std::vector<band::GridRef> refs;
+  std::vector<int2> per[6];
+  std::vector<int> cells[6];
+  for (size_t k = 0; k < grids.size(); ++k) {
+    jxf_grid3d* g = grids[k];
+    if (g->d.boundary != JXF_BND_PEC)
+      return fail(JXF_ERR_INVALID, "grid %zu: a learned band needs PEC-walled grids", k);
+    TRY(band_check_dims(g->d.nx, g->d.ny, g->d.nz));
+    band::GridRef r{};
+    for (int c = 0; c < 6; ++c) r.f[c] = g->f[0][c];
+    r.nx = g->d.nx;
+    r.ny = g->d.ny;
+    r.nz = g->d.nz;
+    refs.push_back(r);
+    band_cells(g->d.nx, g->d.ny, g->d.nz, cells);
+    for (int f = 0; f < 6; ++f)
+      for (int c : cells[f]) per[f].push_back(make_int2(c, (int)k));
+  }
+  std::vector<int2> tc;
+  std::vector<int> tf;
+  band_tiles(per, tc, tf);
+  BandTables n{};
+  int rc = upload(&n.d_grids, refs, tally);
+  if (rc == JXF_OK) rc = upload(&n.d_cells, tc, tally);
+  if (rc == JXF_OK) rc = upload(&n.d_tile_face, tf, tally);
+  if (rc == JXF_OK) rc = dmalloc(&n.d_delta, tc.size() * band::kOut, tally);
+  if (rc != JXF_OK) {
+    band_release(n);
+    return rc;
+  }
+  n.tiles = (int)tf.size();
+  n.ctas = band_ctas(n.tiles, device);
+  n.band = m;
+  t = n;
   return JXF_OK;
 }
 
@@ -2313,43 +2367,21 @@ int jxf_batch3d_set_band(jxf_batch3d* b, jxf_band* m) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
-  b->band = nullptr;
-  b->band_tiles = 0;
+  band_release(b->band);
   if (!m) return JXF_OK;
-  if (m->device != b->device) return fail(JXF_ERR_INVALID, "band and batch on different devices");
-  std::vector<band::GridRef> refs;
-  std::vector<int2> per[6];
-  std::vector<int> cells[6];
-  for (size_t k = 0; k < b->grids.size(); ++k) {
-    jxf_grid3d* g = b->grids[k];
-    if (g->d.boundary != JXF_BND_PEC)
-      return fail(JXF_ERR_INVALID, "grid %zu: a learned band needs PEC-walled grids", k);
-    TRY(band_check_dims(g->d.nx, g->d.ny, g->d.nz));
-    band::GridRef r{};
-    for (int c = 0; c < 6; ++c) r.f[c] = g->f[0][c];
-    r.nx = g->d.nx;
-    r.ny = g->d.ny;
-    r.nz = g->d.nz;
-    refs.push_back(r);
-    band_cells(g->d.nx, g->d.ny, g->d.nz, cells);
-    for (int f = 0; f < 6; ++f)
-      for (int c : cells[f]) per[f].push_back(make_int2(c, (int)k));
-  }
-  std::vector<int2> tc;
-  std::vector<int> tf;
-  band_tiles(per, tc, tf);
-  dfree(b->d_band_grids);
-  dfree(b->d_band_cells);
-  dfree(b->d_band_tile_face);
-  dfree(b->d_band_delta);
-  TRY(upload(&b->d_band_grids, refs, &b->bytes));
-  TRY(upload(&b->d_band_cells, tc, &b->bytes));
-  TRY(upload(&b->d_band_tile_face, tf, &b->bytes));
-  TRY(dmalloc(&b->d_band_delta, tc.size() * band::kOut, &b->bytes));
-  b->band_tiles = (int)tf.size();
-  b->band_ctas = band_ctas(b->band_tiles, b->device);
-  b->band = m;
-  return JXF_OK;
+  return band_attach(b->grids, m, b->device, &b->bytes, b->band);
+}
+
+int jxf_grid3d_set_band(jxf_grid3d* g, jxf_band* m) {
+  if (!g) return fail(JXF_ERR_INVALID, "null grid");
+  DeviceGuard dg(g->d.device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  band_release(g->band);
+  if (!m) return JXF_OK;
+  if (g->path != JXF_PATH_GENERIC || g->slab)
+    return fail(JXF_ERR_INVALID, "a learned band runs on the generic path of a whole grid");
+  std::vector<jxf_grid3d*> one{g};
+  return band_attach(one, m, g->d.device, &g->bytes, g->band);
 }
 
 }  // extern "C"

@@ -36,6 +36,12 @@ class FDTDBatch:
         self._h = h
         self._last_n = 0
         self.band = None
+        learned = [g for g in grids if g._boundary == "learned"]
+        if learned:
+            if len(learned) != len(grids) or any(g._band is not learned[0]._band for g in learned):
+                raise ConfigurationError("a batch with learned boundaries needs every grid "
+                                         "learned, with one shared band")
+            self.set_band(learned[0]._band)
 
     def set_band(self, model) -> None:
         """Attach a learned absorbing band (``LearnedBand``; PEC grids only)

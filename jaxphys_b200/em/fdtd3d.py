@@ -49,6 +49,8 @@ _BOUNDARY = {
     "periodic": nat.BND_PERIODIC,
     "pec": nat.BND_PEC,
     "cpml": nat.BND_CPML,
+    # learned absorbing band: PEC walls plus the band correction after each step
+    "learned": nat.BND_PEC,
 }
 _PATH = {"auto": nat.PATH_AUTO, "generic": nat.PATH_GENERIC, "tma": nat.PATH_TMA}
 
@@ -131,23 +133,28 @@ class EMGrid3D:
         size: Grid dimensions (nx, ny, nz) in cells.
         resolution: Cell size in meters (uniform in all directions).
         boundary: "absorbing" (reference damping layers), "periodic",
-            "pec" (no boundary treatment) or "cpml" (extension).
+            "pec" (no boundary treatment), "cpml" (extension) or "learned"
+            (extension: the outer 3 cell layers are a learned absorbing band,
+            ``jaxphys_b200.em.learned``; generic kernel path).
         pml_layers: Number of damping / CPML layers.
         cpml: CPML grading (boundary="cpml").
         device: CUDA device ordinal (default: torch's current device).
         path: "auto", "tma" or "generic" kernel path.
+        band: boundary="learned": the ``LearnedBand`` to use (default: the
+            shipped weights).
     """
 
     def __init__(
         self,
         size: tuple[int, int, int] = (60, 60, 60),
         resolution: float = 0.01,
-        boundary: Literal["absorbing", "periodic", "pec", "cpml"] = "absorbing",
+        boundary: Literal["absorbing", "periodic", "pec", "cpml", "learned"] = "absorbing",
         pml_layers: int = 8,
         *,
         cpml: CPMLSpec | None = None,
         device: int | None = None,
         path: str = "auto",
+        band=None,
     ) -> None:
         self._nx, self._ny, self._nz = (int(v) for v in size)
         self._dx = resolution
@@ -160,7 +167,8 @@ class EMGrid3D:
         self._probes: list[tuple[int, int, int, int]] = []
         self._cpml = cpml or CPMLSpec()
         self._device = device
-        self._path = path
+        self._path = "generic" if boundary == "learned" else path
+        self._band = band
         self._h = None
         self._h_key = None
         self._dt = None
@@ -290,6 +298,12 @@ class EMGrid3D:
         nat.check(lib.jxf_grid3d_create(C.byref(d), C.byref(h)), "jxf_grid3d_create")
         self._h = h
         self._h_key = key
+        if self._boundary == "learned":
+            from .learned import default_band
+
+            if self._band is None:
+                self._band = default_band(int(dev))
+            nat.check(lib.jxf_grid3d_set_band(h, self._band._h), "jxf_grid3d_set_band")
         self._dt = dt
         self._wave_cap = 0
         self._dirty = True

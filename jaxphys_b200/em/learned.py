@@ -64,6 +64,21 @@ def init_params(seed: int = 0, out_scale: float = 0.1) -> np.ndarray:
     return P
 
 
+WEIGHTS = __import__("pathlib").Path(__file__).resolve().parent / "band_weights.npz"
+_DEFAULT: dict = {}
+
+
+def default_band(device: int | None = None) -> "LearnedBand":
+    """The shipped band (``band_weights.npz``, made by ``train_band(seed=0)``),
+    one shared instance per device."""
+    import torch
+
+    dev = torch.cuda.current_device() if device is None else int(device)
+    if dev not in _DEFAULT:
+        _DEFAULT[dev] = LearnedBand.load(WEIGHTS, device=dev)
+    return _DEFAULT[dev]
+
+
 def _field_ptrs(g: EMGrid3D):
     lib = nat.load()
     out = (C.c_void_p * 6)()

@@ -214,3 +214,42 @@ def test_onpolicy_collection_appends_rows(cuda):
     x, t, w = m.dataset(0)
     assert np.all(np.isfinite(x)) and np.all(np.isfinite(t)) and np.all(w >= 0)
     m.close()
+
+
+def test_learned_boundary_grid_matches_batch(cuda):
+    """EMGrid3D(boundary="learned") steps through the single-grid path with
+    the band attached to the handle; a batch of one PEC grid with the same band
+    gives bit-identical fields and probe traces."""
+    import torch
+
+    from jaxphys_b200 import EMGrid3D, PointSource3D
+    from jaxphys_b200.em.batch import FDTDBatch
+    from jaxphys_b200.em.fdtd3d import COMPONENTS
+    from jaxphys_b200.em.learned import default_band
+
+    def make(boundary):
+        g = EMGrid3D((22, 20, 24), resolution=1.0, boundary=boundary, path="generic")
+        dt = g.default_dt()
+        g.add_source(PointSource3D(frequency=0.05 / dt, position=(11, 10, 12), polarization="y",
+                                   waveform="gauss_sine", width_steps=12.0))
+        g.add_probe((4, 5, 6), "ey")
+        g.add_probe((18, 2, 20), "hz")
+        g.prepare()
+        return g
+
+    a = make("learned")
+    ta = a.run(120)
+    b = make("pec")
+    bb = FDTDBatch([b])
+    bb.set_band(default_band())
+    tb = bb.run(120, use_graph=True)[0]
+    assert torch.equal(ta, tb)
+    for c in COMPONENTS:
+        assert torch.equal(a.field(c), b.field(c)), c
+    assert torch.isfinite(a.field("ey")).all()
+    # and the learned batch of learned grids attaches the band itself
+    c = make("learned")
+    bc = FDTDBatch([c])
+    assert bc.band is a._band
+    h = a.simulate(t_span=(0.0, 60 * a.default_dt()), save_every=20)
+    assert torch.isfinite(h.ey).all()
