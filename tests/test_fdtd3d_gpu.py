@@ -59,6 +59,16 @@ def test_tma_bitwise_equals_generic(cuda, case):
         assert np.array_equal(to_np(getattr(a, k)), to_np(getattr(b, k))), k
 
 
+# launch shapes in the library's TMA registry (checked against the library below)
+N_TMA_CONFIGS = 9
+
+
+def test_tma_registry_size(cuda):
+    from jaxphys_b200 import _native as nat
+
+    assert nat.load().jxf_num_tma_configs() == N_TMA_CONFIGS
+
+
 def _cpml_grid(path, size, eps, sources, probes, n_pml=6, cpml=None):
     from jaxphys_b200 import CPMLSpec, EMGrid3D, PointSource3D
 
@@ -141,7 +151,7 @@ def test_cpml_tma_bitwise_generic_with_kappa_alpha(cuda):
     _assert_fields([res[0][k] for k in COMPS], o.f, tol=1e-6, what="vs FP32")
 
 
-@pytest.mark.parametrize("cfg", range(5))
+@pytest.mark.parametrize("cfg", range(N_TMA_CONFIGS))
 @pytest.mark.parametrize("chunk", [1, 3, 64])
 def test_every_launch_shape_bitwise(cuda, cfg, chunk):
     """Every TMA tile shape and x-chunk (including 1-plane chunks, ragged tiles
@@ -167,7 +177,7 @@ def test_every_launch_shape_bitwise(cuda, cfg, chunk):
     assert np.array_equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("cfg", range(5))
+@pytest.mark.parametrize("cfg", range(N_TMA_CONFIGS))
 def test_absorbing_launch_shapes_bitwise(cuda, cfg):
     from jaxphys_b200 import EMGrid3D, PointSource3D
     from jaxphys_b200 import _native as nat
