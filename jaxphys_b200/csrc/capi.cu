@@ -230,7 +230,8 @@ const std::vector<TmaConfig>& tma_configs() {
       // small-grid shapes: 128-thread blocks (more blocks per SM, less
       // shared memory per block), 3-stage ring
       make_cfg<32, 4, 1, 4>(),  make_cfg<32, 8, 2, 4>(),  make_cfg<32, 8, 1, 3>(),
-      make_cfg<64, 4, 1, 3>(),
+      make_cfg<64, 4, 1, 3>(),  make_cfg<32, 4, 1, 3>(),  make_cfg<16, 8, 1, 3>(),
+      make_cfg<64, 8, 1, 3>(),
   };
   return cfgs;
 }

@@ -60,7 +60,7 @@ def test_tma_bitwise_equals_generic(cuda, case):
 
 
 # launch shapes in the library's TMA registry (checked against the library below)
-N_TMA_CONFIGS = 9
+N_TMA_CONFIGS = 12
 
 
 def test_tma_registry_size(cuda):
