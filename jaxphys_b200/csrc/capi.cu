@@ -1836,7 +1836,10 @@ int band_owner(int x, int y, int z, int nx, int ny, int nz) {
   return (b == (a + 1) % 3) ? 2 * a + sd[0] : 2 * b + sd[1];
 }
 
-// Outer-layer cells of an nx*ny*nz grid, per owning face, ascending.
+// Outer-layer cells of an nx*ny*nz grid, per owning face: x and y faces in
+// ascending cell order (neighbouring lanes read neighbouring z), z faces in
+// (y, x) order (neighbouring lanes step along x, the stencil's tangent axis,
+// so they share the stencil rows x-1, x, x+1).
 void band_cells(int nx, int ny, int nz, std::vector<int> out[6]) {
   for (int f = 0; f < 6; ++f) out[f].clear();
   for (int x = 0; x < nx; ++x)
@@ -1847,6 +1850,11 @@ void band_cells(int nx, int ny, int nz, std::vector<int> out[6]) {
         if (f >= 0) out[f].push_back((x * ny + y) * nz + z);
       }
     }
+  for (int f = 4; f < 6; ++f)
+    std::stable_sort(out[f].begin(), out[f].end(), [&](int a, int b) {
+      const int ya = (a / nz) % ny, yb = (b / nz) % ny;
+      return ya != yb ? ya < yb : a < b;
+    });
 }
 
 int band_check_dims(int nx, int ny, int nz) {

@@ -184,7 +184,8 @@ def owner(x: int, y: int, z: int, n) -> int:
 
 
 def band_cells(n) -> list[np.ndarray]:
-    """Outer-layer cell indices per owning face, ascending."""
+    """Outer-layer cell indices per owning face: x and y faces ascending, z
+    faces ordered by (y, x) (the order the kernels process them in)."""
     nx, ny, nz = n
     out = [[] for _ in range(6)]
     for x in range(nx):
@@ -195,7 +196,11 @@ def band_cells(n) -> list[np.ndarray]:
                 f = owner(x, y, z, n)
                 if f >= 0:
                     out[f].append((x * ny + y) * nz + z)
-    return [np.asarray(v, dtype=np.int64) for v in out]
+    res = [np.asarray(v, dtype=np.int64) for v in out]
+    for f in (4, 5):
+        c = res[f]
+        res[f] = c[np.lexsort((c, (c // nz) % ny))]
+    return res
 
 
 def features(fields, cells: np.ndarray, face: int):
