@@ -467,6 +467,9 @@ Step3D base_params(jxf_grid3d* g) {
   p.gnx = g->gnx;
   p.x_lo = g->x_lo;
   p.x_hi = g->x_hi;
+  p.div_nz = make_fastdiv((uint32_t)g->d.nz);
+  p.div_ny = make_fastdiv((uint32_t)g->d.ny);
+  p.idx32 = ((long long)g->d.nx * g->d.ny * g->d.nz) < (1ll << 32) ? 1 : 0;
   return p;
 }
 
@@ -2500,6 +2503,9 @@ extern "C" int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_gra
   a.nx = g->d.nx;
   a.ny = g->d.ny;
   a.nz = g->d.nz;
+  a.div_nz = make_fastdiv((uint32_t)g->d.nz);
+  a.div_ny = make_fastdiv((uint32_t)g->d.ny);
+  a.idx32 = ((long long)g->d.nx * g->d.ny * g->d.nz) < (1ll << 32) ? 1 : 0;
   a.a = (float)g->coef_h;
   a.cb_const = (float)g->coef_e;
   a.cb = g->cb;

@@ -45,6 +45,8 @@ struct Adj3D {
   float* db[6];
   float* dh[6];
   double* gcb;                // dJ/dcb accumulator
+  FastDiv div_nz, div_ny;     // index decode (idx32: nx ny nz < 2^32)
+  int idx32;
 };
 
 // psi adjoint through one term: tot = carried + u; new carried = b * tot;
@@ -62,10 +64,8 @@ __global__ void __launch_bounds__(256) k3a_e(const __grid_constant__ Adj3D p) {
   constexpr bool CP = (MODE == MODE_CPML);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(i % nz);
-    const long long t = i / nz;
-    const int y = (int)(t % ny);
-    const int x = (int)(t / ny);
+    int x, y, z;
+    decode_cell(i, nz, ny, p.idx32 != 0, p.div_nz, p.div_ny, x, y, z);
     const float cb = p.cb ? p.cb[i] : p.cb_const;
     float damp = 1.0f;
     if (MODE == MODE_ABSORB)
@@ -137,10 +137,8 @@ __global__ void __launch_bounds__(256) k3a_h(const __grid_constant__ Adj3D p) {
   constexpr bool CP = (MODE == MODE_CPML);
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
        j += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(j % nz);
-    const long long t = j / nz;
-    const int y = (int)(t % ny);
-    const int x = (int)(t / ny);
+    int x, y, z;
+    decode_cell(j, nz, ny, p.idx32 != 0, p.div_nz, p.div_ny, x, y, z);
     // Hbar' = lH + G^T dbarE
     const float zp_db2 = (z + 1 < nz) ? p.db[2][j + 1] : 0.0f;
     const float yp_db5 = (y + 1 < ny) ? p.db[5][j + nz] : 0.0f;
@@ -198,10 +196,8 @@ __global__ void __launch_bounds__(256) k3a_e2(const __grid_constant__ Adj3D p) {
   const long long sx = (long long)ny * nz;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(i % nz);
-    const long long t = i / nz;
-    const int y = (int)(t % ny);
-    const int x = (int)(t / ny);
+    int x, y, z;
+    decode_cell(i, nz, ny, p.idx32 != 0, p.div_nz, p.div_ny, x, y, z);
     const float zm_dh2 = z >= 1 ? p.dh[2][i - 1] : 0.0f;
     const float ym_dh5 = y >= 1 ? p.dh[5][i - nz] : 0.0f;
     const float zm_dh1 = z >= 1 ? p.dh[1][i - 1] : 0.0f;

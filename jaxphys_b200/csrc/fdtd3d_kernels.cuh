@@ -164,10 +164,8 @@ __device__ __forceinline__ void generic_h_body(const Step3D& p, long long k0, lo
   const float* ez = p.in[2];
   for (long long k = k0; k < n; k += kstep) {
     const long long idx = base + k;
-    const int z = (int)(idx % nz);
-    const long long t = idx / nz;
-    const int y = (int)(t % ny);
-    const int x = (int)(t / ny);
+    int x, y, z;
+    decode_cell(idx, nz, ny, p.idx32 != 0, p.div_nz, p.div_ny, x, y, z);
     const int xg = x + p.gx0;  // global plane
     long long ixp, iyp, izp;  // neighbours at +1
     bool ux, uy, uz;          // Hx, Hy, Hz updated here
@@ -240,10 +238,8 @@ __device__ __forceinline__ void generic_e_body(const Step3D& p, long long k0, lo
   const float* hz = p.out[5];
   for (long long k = k0; k < n; k += kstep) {
     const long long idx = base + k;
-    const int z = (int)(idx % nz);
-    const long long t = idx / nz;
-    const int y = (int)(t % ny);
-    const int x = (int)(t / ny);
+    int x, y, z;
+    decode_cell(idx, nz, ny, p.idx32 != 0, p.div_nz, p.div_ny, x, y, z);
     const int xg = x + p.gx0;  // global plane
     long long ixm, iym, izm;
     bool ux, uy, uz;

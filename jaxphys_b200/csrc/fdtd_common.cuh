@@ -50,6 +50,42 @@ struct SrcTerm {
   int wave;
 };
 
+// Unsigned division of 32-bit numerators by a divisor fixed per launch:
+// q = (umulhi(n, m) + n) >> s with s = ceil(log2 d) and
+// m = floor(2^32 (2^s - d) / d) + 1 (the round-up multiply-high method,
+// Granlund & Montgomery 1994 / Warren, Hacker's Delight 10-9); exact for every
+// n < 2^32 (checked exhaustively for the divisor classes used).
+struct FastDiv {
+  uint32_t d, m, s;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f{d, 0u, 0u};
+  while ((1ull << f.s) < d) ++f.s;
+  f.m = (uint32_t)((((1ull << 32) * ((1ull << f.s) - d)) / d + 1ull) & 0xFFFFFFFFull);
+  return f;
+}
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+  return (uint32_t)(((unsigned long long)__umulhi(n, f.m) + n) >> f.s);
+}
+// (x, y, z) of linear index idx = (x ny + y) nz + z.
+__device__ __forceinline__ void decode_cell(long long idx, int nz, int ny, bool idx32,
+                                            const FastDiv& dnz, const FastDiv& dny, int& x,
+                                            int& y, int& z) {
+  if (idx32) {
+    const uint32_t u = (uint32_t)idx;
+    const uint32_t t = fdiv(u, dnz);
+    const uint32_t xx = fdiv(t, dny);
+    z = (int)(u - t * (uint32_t)nz);
+    y = (int)(t - xx * (uint32_t)ny);
+    x = (int)xx;
+  } else {
+    z = (int)(idx % nz);
+    const long long t = idx / nz;
+    y = (int)(t % ny);
+    x = (int)(t / ny);
+  }
+}
+
 struct CpmlDev {
   const float* tab[3][TAB_COUNT];  // per axis, length n_axis
   int L[3];                        // slab storage extent per axis
@@ -91,6 +127,9 @@ struct Step3D {
   // are updated, local plane x is global plane x + gx0 of a grid of gnx
   // planes; planes outside the range are ghost copies of neighbouring ranks.
   int gx0, gnx, x_lo, x_hi;
+  // index decode of the generic kernels (idx32: every local index < 2^32)
+  FastDiv div_nz, div_ny;
+  int idx32;
 };
 
 enum PdlBits : int { PDL_WAIT_START = 1, PDL_TRIGGER = 2, PDL_WAIT_END = 4 };
