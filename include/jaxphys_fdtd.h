@@ -206,9 +206,9 @@ int jxf_batch3d_probes(jxf_batch3d* b, int32_t grid, int32_t n_steps, float* dst
  *   jxf_band_eval      outputs for given normalised feature rows (testing).
  *   jxf_batch3d_set_band / jxf_grid3d_set_band attach a band to a batch of
  *                      PEC grids / to one PEC grid on the generic path (NULL
- *                      detaches); every later step applies it.  Detach or
- *                      destroy those grids and batches before destroying
- *                      the band. */
+ *                      detaches); every later step applies it.
+ *                      jxf_band_destroy fails (JXF_ERR_INVALID) while a grid
+ *                      or batch still has the band attached. */
 #define JXF_BAND_PARAMS 9360
 #define JXF_BAND_FACES 6
 #define JXF_BAND_FEATURES 54

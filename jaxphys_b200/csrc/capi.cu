@@ -1802,6 +1802,7 @@ struct jxf_band {
   long long cap[6] = {};
   int* d_cells = nullptr;  // collect scratch
   size_t cells_cap = 0;
+  int attached = 0;        // grids and batches applying this band
 };
 
 namespace {
@@ -1889,6 +1890,7 @@ int band_launch(const BandTables& t, cudaStream_t st) {
 }
 
 void band_release(BandTables& t) {
+  if (t.band) t.band->attached -= 1;
   dfree(t.d_grids);
   dfree(t.d_cells);
   dfree(t.d_tile_face);
@@ -2032,6 +2034,7 @@ int band_attach(const std::vector<jxf_grid3d*>& grids, jxf_band* m, int device, 
   n.tiles = (int)tf.size();
   n.ctas = band_ctas(n.tiles, device);
   n.band = m;
+  m->attached += 1;
   t = n;
   return JXF_OK;
 }
@@ -2091,6 +2094,9 @@ int jxf_band_create(int32_t device, jxf_band** out) {
 
 int jxf_band_destroy(jxf_band* m) {
   if (!m) return JXF_OK;
+  if (m->attached > 0)
+    return fail(JXF_ERR_INVALID, "the band is still attached to %d grid(s) or batch(es)",
+                m->attached);
   DeviceGuard dg(m->device);
   cudaDeviceSynchronize();
   dfree(m->d_params);

@@ -103,8 +103,9 @@ class LearnedBand:
         self.params = init_params(seed) if params is None else params
 
     def close(self) -> None:
+        """Free the device copy (refused while a grid or batch still uses it)."""
         if self._h is not None:
-            nat.load().jxf_band_destroy(self._h)
+            nat.check(nat.load().jxf_band_destroy(self._h), "jxf_band_destroy")
             self._h = None
 
     def __del__(self):  # pragma: no cover

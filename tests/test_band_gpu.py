@@ -253,3 +253,22 @@ def test_learned_boundary_grid_matches_batch(cuda):
     assert bc.band is a._band
     h = a.simulate(t_span=(0.0, 60 * a.default_dt()), save_every=20)
     assert torch.isfinite(h.ey).all()
+
+
+def test_band_destroy_refused_while_attached(cuda):
+    from jaxphys_b200 import EMGrid3D
+    from jaxphys_b200.em.batch import FDTDBatch
+    from jaxphys_b200.em.learned import LearnedBand
+    from jaxphys_b200.exceptions import NeurosimError
+
+    m = LearnedBand(seed=2)
+    g = EMGrid3D((12, 12, 12), resolution=1.0, boundary="learned", band=m)
+    g.prepare()
+    b = FDTDBatch([g])
+    with pytest.raises(NeurosimError):
+        m.close()
+    b.close()
+    with pytest.raises(NeurosimError):   # the grid still holds it
+        m.close()
+    g._release()
+    m.close()
