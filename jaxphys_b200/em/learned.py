@@ -539,8 +539,24 @@ def _main(argv=None) -> None:
     ap.add_argument("--size", type=int, default=120, help="interior side")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--train", type=int, default=0, metavar="ITERS",
+                    help="instead: collect CPML traces of one box and run ITERS Adam steps")
     a = ap.parse_args(argv)
     rng = np.random.default_rng(a.seed)
+    if a.train > 0:
+        m = LearnedBand(seed=a.seed)
+        collect_traces(m, random_case(rng, (32, 30, 34), eps_range=(1.0, 6.0)), n_steps=200,
+                       noise=0.03, seed=a.seed)
+        rows = int(m.dataset_size().sum())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = m.train(a.train, batch_rows=8192, lr=1e-3, seed=a.seed)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        print(f"{rows} rows; {a.train} Adam steps of 6 x 8192 rows in {dt:.3f} s "
+              f"({a.train * 6 * 8192 / dt / 1e6:.1f} M rows/s); loss {loss[0]:.4g} -> {loss[-1]:.4g}")
+        m.close()
+        return
     cases = [random_case(rng, (a.size,) * 3, eps_range=(1.0, 6.0)) for _ in range(a.grids)]
     grids = []
     for c in cases:
