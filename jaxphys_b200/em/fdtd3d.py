@@ -494,12 +494,20 @@ class EMGrid3D:
         dt: float | None = None,
         save_every: int = 20,
         output: Literal["torch", "numpy"] = "torch",
+        history: Literal["device", "host"] = "device",
     ) -> EMFieldHistory3D:
         """Run the 3D FDTD simulation (fdtd3d.py:169-417).
 
         Returns the frames the reference keeps: states after steps
         1, 1+s, 1+2s, ... (s = save_every; every step when s <= 1) with their
         times t_start + k*dt + dt.
+
+        history="device" keeps the frames in device memory (torch tensors on
+        the GPU).  history="host" streams them into pinned host memory as they
+        are produced: each frame is copied into one of two device staging
+        slots and from there to the host on a side stream while the next
+        steps run, so device memory holds two frames whatever the number of
+        frames (the reference materialises every step, fdtd3d.py:371-404).
         """
         import torch
 
@@ -519,9 +527,21 @@ class EMGrid3D:
         stride = save_every if save_every > 1 else 1
         saved = list(range(0, max(n_steps, 0), stride))
         dev = f"cuda:{self._h_key[1]}"
-        hist = [torch.empty((len(saved),) + self.size, dtype=torch.float32, device=dev)
-                for _ in COMPONENTS]
+        if history not in ("device", "host"):
+            raise ConfigurationError(f"history must be 'device' or 'host', got {history!r}")
+        to_host = history == "host"
+        if to_host:
+            hist = [torch.empty((len(saved),) + self.size, dtype=torch.float32, pin_memory=True)
+                    for _ in COMPONENTS]
+            stage = [torch.empty((6,) + self.size, dtype=torch.float32, device=dev)
+                     for _ in range(2)]
+            copy_stream = torch.cuda.Stream(device=dev)
+            slot_free = [None, None]
+        else:
+            hist = [torch.empty((len(saved),) + self.size, dtype=torch.float32, device=dev)
+                    for _ in COMPONENTS]
         lib = nat.load()
+        main = torch.cuda.current_stream(dev)
         st = nat.stream_handle()
         self._ensure_waves(max(n_steps, 1))
         done = 0
@@ -529,11 +549,29 @@ class EMGrid3D:
             if k + 1 > done:
                 nat.check(lib.jxf_grid3d_step(self._h, k + 1 - done, None, st), "jxf_grid3d_step")
                 done = k + 1
+            if not to_host:
+                for c in range(6):
+                    nat.check(lib.jxf_grid3d_get_field(self._h, c, hist[c][s].data_ptr(), 0, st),
+                              "get_field")
+                continue
+            slot = s % 2
+            if slot_free[slot] is not None:
+                main.wait_event(slot_free[slot])  # its previous frame has reached the host
             for c in range(6):
-                nat.check(lib.jxf_grid3d_get_field(self._h, c, hist[c][s].data_ptr(), 0, st),
+                nat.check(lib.jxf_grid3d_get_field(self._h, c, stage[slot][c].data_ptr(), 0, st),
                           "get_field")
+            ready = torch.cuda.Event()
+            ready.record(main)
+            copy_stream.wait_event(ready)
+            with torch.cuda.stream(copy_stream):
+                for c in range(6):
+                    hist[c][s].copy_(stage[slot][c], non_blocking=True)
+                slot_free[slot] = torch.cuda.Event()
+                slot_free[slot].record(copy_stream)
         if n_steps > done:
             nat.check(lib.jxf_grid3d_step(self._h, n_steps - done, None, st), "jxf_grid3d_step")
+        if to_host:
+            copy_stream.synchronize()
         self.check(finite=True)
         t = np.array([t_start + k * dt + dt for k in saved], dtype=np.float64)
         gx = np.arange(nx) * dx

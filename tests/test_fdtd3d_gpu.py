@@ -390,3 +390,24 @@ def test_grid_coordinates(cuda):
     f = grid.simulate(t_span=(0, 1e-10), save_every=5)
     assert f.grid_x.shape == (16,)
     assert float(f.grid_x[1] - f.grid_x[0]) == pytest.approx(0.02)
+
+
+def test_history_streamed_to_host_equals_device(cuda):
+    """simulate(history="host") streams frames to pinned host memory through
+    two device staging slots; the frames equal the device-resident history."""
+    from jaxphys_b200 import EMGrid3D, PointSource3D
+
+    def make():
+        g = EMGrid3D(size=(20, 24, 28), resolution=0.01, boundary="absorbing", pml_layers=4)
+        g.add_source(PointSource3D(frequency=5e9, position=(10, 12, 14)))
+        return g
+
+    t_span = (0.0, 60 * make().default_dt())
+    a = make().simulate(t_span, save_every=7)
+    b = make().simulate(t_span, save_every=7, history="host")
+    assert not b.ez.is_cuda and b.ez.is_pinned()
+    np.testing.assert_array_equal(to_np(a.t), to_np(b.t))
+    for k in COMPS:
+        assert np.array_equal(to_np(getattr(a, k)), to_np(getattr(b, k))), k
+    c = make().simulate(t_span, save_every=7, history="host", output="numpy")
+    assert isinstance(c.hx, np.ndarray) and np.array_equal(c.hx, to_np(a.hx))
