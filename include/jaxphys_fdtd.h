@@ -95,6 +95,11 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out);
  * cfg < 0 returns to autotuning (which runs on the first step otherwise). */
 int jxf_num_tma_configs(void);
 int jxf_grid3d_set_launch(jxf_grid3d* g, int32_t cfg, int32_t x_chunk);
+/* CPML grids on the TMA path: on != 0 runs the shell blocks that touch the
+ * psi slab of one axis only on kernels specialised for that axis (4 psi
+ * arrays instead of 12, smaller shared memory); the autotuner chooses it per
+ * grid shape, this pins it (with jxf_grid3d_set_launch). */
+int jxf_grid3d_set_axis_split(jxf_grid3d* g, int32_t on);
 
 /* Relative permittivity, replaces _build_epsilon_r (fdtd3d.py:132-137) and
  * the per-cell factor (dt_eps_dx / eps_r) of fdtd3d.py:299,336,345,354.

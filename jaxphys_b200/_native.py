@@ -97,6 +97,7 @@ SIGNATURES = {
     "jxf_grid3d_destroy": (C.c_int, [_vp]),
     "jxf_grid3d_get_info": (C.c_int, [_vp, C.POINTER(Grid3DInfo)]),
     "jxf_grid3d_set_launch": (C.c_int, [_vp, _i32, _i32]),
+    "jxf_grid3d_set_axis_split": (C.c_int, [_vp, _i32]),
     "jxf_grid3d_set_eps_host": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_set_eps_device": (C.c_int, [_vp, _vp, _vp]),
     "jxf_grid3d_set_sources": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),

@@ -202,6 +202,9 @@ struct TmaConfig {
   int threads;
   size_t smem[2];     // [mode: 0 absorb, 1 cpml]
   TmaKernel k[3][2];  // [0 absorb, 1 cpml (kappa = 1), 2 cpml (kappa > 1)][cbarr]
+  // CPML (kappa = 1) for blocks touching the slab of one axis only [x, y, z][cbarr]
+  size_t smem_ax[3];
+  TmaKernel kax[3][2];
 };
 
 template <int TZ, int TY, int RY, int ST>
@@ -220,6 +223,15 @@ TmaConfig make_cfg() {
   c.k[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false>;
   c.k[2][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, true>;
   c.k[2][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, true>;
+  c.smem_ax[0] = TmaLayout<TZ, TY, RY, ST, true, true, 1>::SMEM_BYTES;
+  c.smem_ax[1] = TmaLayout<TZ, TY, RY, ST, true, true, 2>::SMEM_BYTES;
+  c.smem_ax[2] = TmaLayout<TZ, TY, RY, ST, true, true, 4>::SMEM_BYTES;
+  c.kax[0][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 1>;
+  c.kax[0][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 1>;
+  c.kax[1][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 2>;
+  c.kax[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 2>;
+  c.kax[2][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 4>;
+  c.kax[2][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 4>;
   return c;
 }
 
@@ -236,9 +248,9 @@ const std::vector<TmaConfig>& tma_configs() {
   return cfgs;
 }
 
-// autotune results: (nx, ny, nz, mode, cbarr) -> (cfg index, x_chunk)
+// autotune results: (nx, ny, nz, mode, cbarr) -> (cfg index, x_chunk, axis split)
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int>, std::tuple<int, int, int>> g_tune_cache;
 
 }  // namespace
 
@@ -308,9 +320,13 @@ struct jxf_grid3d {
   int* d_count = nullptr;
   // CPML region split: blocks that touch a psi slab (shell) run the CPML
   // kernel, the others the plain kernel (compact block lists per launch shape)
-  int* d_shell = nullptr;
+  int* d_shell = nullptr;     // shell blocks touching slabs of several axes
+  int* d_shell_ax[3] = {};    // shell blocks touching the slab of one axis (x, y, z)
   int* d_inner = nullptr;
   int n_shell = 0, n_inner = 0;
+  int n_shell_ax[3] = {0, 0, 0};
+  int axis_split = 0;         // run single-axis shell blocks on the specialised kernels
+  int split_axes = -1;        // axis_split the current block lists were built for
   int split_cfg = -1, split_chunk = -1;
   bool use_pdl = true;  // programmatic dependent launch between step kernels
   // adjoint (sqrt(T) checkpointing): checkpoints of the full state every
@@ -485,7 +501,7 @@ void set_io(jxf_grid3d* g, Step3D& p, int in_set, int out_set) {
 }
 
 int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStream_t st,
-               int list_count, bool plain = false) {
+               int list_count, bool plain = false, int axis = -1) {
   // The boxes of the tensor maps must be the ones this config's kernel expects
   // (the mbarrier transaction count is derived from them).
   if (!g->maps_ok || g->maps_cfg != cfg)
@@ -496,11 +512,22 @@ int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStr
   const int mi = cpml ? 1 : 0;
   const int ki = cpml ? (g->kappa ? 2 : 1) : 0;
   TmaKernel k = c.k[ki][g->cb ? 1 : 0];
-  const size_t smem = c.smem[mi];
-  static std::mutex mu;
+  size_t smem = c.smem[mi];
+  if (cpml && axis >= 0) {  // single-axis shell blocks (kappa = 1 only)
+    k = c.kax[axis][g->cb ? 1 : 0];
+    smem = c.smem_ax[axis];
+  }
   {
+    // the shared-memory opt-in is set once per kernel and device (a driver
+    // call per launch would make small steps host bound)
+    static std::mutex mu;
+    static std::map<std::pair<TmaKernel, int>, size_t> done;
     std::lock_guard<std::mutex> lk(mu);
-    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    size_t& have = done[{k, g->d.device}];
+    if (have < smem) {
+      CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      have = smem;
+    }
   }
   p.x_chunk = chunk;
   p.ntiles_z = (g->d.nz + c.tz - 1) / c.tz;
@@ -541,38 +568,52 @@ bool range_clear(int lo, int hi, int n, int P) {
 }
 
 int build_split(jxf_grid3d* g, int cfg, int chunk) {
-  if (g->split_cfg == cfg && g->split_chunk == chunk) return JXF_OK;
+  if (g->split_cfg == cfg && g->split_chunk == chunk && g->split_axes == g->axis_split)
+    return JXF_OK;
   const TmaConfig& c = tma_configs()[cfg];
   const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
   const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
   const int nch = (nx + chunk - 1) / chunk;
-  std::vector<int> shell, inner;
+  std::vector<int> shell, inner, axl[3];
+  const bool axis_split = g->axis_split != 0;
   for (int ch = 0; ch < nch; ++ch)
     for (int ty = 0; ty < nty; ++ty)
       for (int tz = 0; tz < ntz; ++tz) {
         const int z0 = tz * c.tz, y0 = ty * c.ty, xb = ch * chunk;
         const int xe = std::min(xb + chunk, nx);
         // cells of the tile, its halo row / column, and the warm-up plane
-        const bool clear = range_clear(z0 - 1, z0 + c.tz - 1, nz, g->P[2]) &&
-                           range_clear(y0 - 1, y0 + c.ty - 1, ny, g->P[1]) &&
-                           range_clear(xb - 1, xe - 1, nx, g->P[0]);
-        std::vector<int>& v = clear ? inner : shell;
-        v.push_back(tz);
-        v.push_back(ty);
-        v.push_back(ch);
+        const bool cz = range_clear(z0 - 1, z0 + c.tz - 1, nz, g->P[2]);
+        const bool cy = range_clear(y0 - 1, y0 + c.ty - 1, ny, g->P[1]);
+        const bool cx = range_clear(xb - 1, xe - 1, nx, g->P[0]);
+        const int touched = (cx ? 0 : 1) + (cy ? 0 : 1) + (cz ? 0 : 1);
+        std::vector<int>* v = &shell;
+        if (touched == 0) v = &inner;
+        else if (touched == 1 && !g->kappa && axis_split) v = &axl[!cx ? 0 : (!cy ? 1 : 2)];
+        v->push_back(tz);
+        v->push_back(ty);
+        v->push_back(ch);
       }
   TRY(upload(&g->d_shell, shell, &g->bytes));
   TRY(upload(&g->d_inner, inner, &g->bytes));
+  for (int a = 0; a < 3; ++a) {
+    TRY(upload(&g->d_shell_ax[a], axl[a], &g->bytes));
+    g->n_shell_ax[a] = (int)axl[a].size() / 3;
+  }
   g->n_shell = (int)shell.size() / 3;
   g->n_inner = (int)inner.size() / 3;
   g->split_cfg = cfg;
   g->split_chunk = chunk;
+  g->split_axes = g->axis_split;
   return JXF_OK;
 }
 
 // One leapfrog step on the TMA path.  CPML grids: the CPML kernel over the
-// shell blocks, then the plain kernel over the interior blocks (disjoint
-// outputs, both read the same input set).
+// shell blocks that touch the slabs of several axes, the single-axis CPML
+// variants over the blocks that touch one axis's slab, then the plain kernel
+// over the interior blocks (disjoint outputs, all read the same input set).
+// Programmatic dependent launch chains them: the first launch waits for the
+// previous step, each later one starts beside its predecessor and waits for
+// it before exiting, so the last one's completion covers the whole step.
 int launch_step(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStream_t st) {
   p.pdl = g->use_pdl ? (PDL_WAIT_START | PDL_TRIGGER) : 0;
   if (g->mode != MODE_CPML) {
@@ -580,18 +621,28 @@ int launch_step(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaSt
     return launch_tma(g, cfg, chunk, p, in_set, st, -1);
   }
   TRY(build_split(g, cfg, chunk));
-  if (g->n_shell > 0) {
-    p.blk_list = g->d_shell;
-    TRY(launch_tma(g, cfg, chunk, p, in_set, st, g->n_shell));
-  }
-  if (g->n_inner > 0) {
+  struct Part {
+    const int* list;
+    int n;
+    bool plain;
+    int axis;
+  };
+  const Part parts[5] = {{g->d_shell, g->n_shell, false, -1},
+                         {g->d_shell_ax[0], g->n_shell_ax[0], false, 0},
+                         {g->d_shell_ax[1], g->n_shell_ax[1], false, 1},
+                         {g->d_shell_ax[2], g->n_shell_ax[2], false, 2},
+                         {g->d_inner, g->n_inner, true, -1}};
+  bool first = true;
+  for (const Part& part : parts) {
+    if (part.n <= 0) continue;
     Step3D q = p;
-    q.blk_list = g->d_inner;
-    q.probe_out = (g->n_shell > 0) ? nullptr : p.probe_out;
-    // runs beside the shell kernel (it was released after the shell kernel
-    // had waited for the previous step) and waits for it before exiting
-    if (g->use_pdl && g->n_shell > 0) q.pdl = PDL_TRIGGER | PDL_WAIT_END;
-    TRY(launch_tma(g, cfg, chunk, q, in_set, st, g->n_inner, /*plain=*/true));
+    q.blk_list = part.list;
+    if (!first) {
+      q.probe_out = nullptr;
+      if (g->use_pdl) q.pdl = PDL_TRIGGER | PDL_WAIT_END;
+    }
+    TRY(launch_tma(g, cfg, chunk, q, in_set, st, part.n, part.plain, part.axis));
+    first = false;
   }
   return JXF_OK;
 }
@@ -601,66 +652,90 @@ int heuristic_tune(jxf_grid3d* g) {
   const long long cells = g->n;
   g->cfg = 0;
   g->x_chunk = cells >= (1LL << 24) ? 64 : (cells >= (1LL << 21) ? 16 : 8);
+  g->axis_split = cells >= (1LL << 25) ? 1 : 0;
   return JXF_OK;
 }
 
-// Time every (config, chunk) on A -> B launches (the state in A and the step
-// counter are untouched, probes off) and keep the fastest.
+// JXF_AXIS_SPLIT=0/1 forces the single-axis shell split off / on.
+int axis_split_override() {
+  const char* e = std::getenv("JXF_AXIS_SPLIT");
+  return e ? (std::atoi(e) != 0 ? 1 : 0) : -1;
+}
+
+// Time every (config, chunk, axis split) on A -> B launches (the state in A
+// and the step counter are untouched, probes off) and keep the fastest.
 int autotune(jxf_grid3d* g, cudaStream_t st) {
   const auto key =
       std::make_tuple(g->d.nx, g->d.ny, g->d.nz, g->mode * 2 + (g->kappa ? 1 : 0), g->cb ? 1 : 0);
+  const int split_env = axis_split_override();
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      g->cfg = it->second.first;
-      g->x_chunk = it->second.second;
+      g->cfg = std::get<0>(it->second);
+      g->x_chunk = std::get<1>(it->second);
+      g->axis_split = std::get<2>(it->second);
       return JXF_OK;
     }
   }
   const char* env = std::getenv("JXF_AUTOTUNE");
   const bool enabled = !(env && env[0] == '0');
-  const char* forced = std::getenv("JXF_LAUNCH");  // "cfg,chunk": pin the launch shape
-  int fc = -1, fk = -1;
-  if (forced && std::sscanf(forced, "%d,%d", &fc, &fk) == 2 && fc >= 0 &&
+  // "cfg,chunk[,split]": pin the launch shape (split defaults to off)
+  const char* forced = std::getenv("JXF_LAUNCH");
+  int fc = -1, fk = -1, fs = 0;
+  if (forced && std::sscanf(forced, "%d,%d,%d", &fc, &fk, &fs) >= 2 && fc >= 0 &&
       fc < (int)tma_configs().size() && fk >= 1) {
     g->cfg = fc;
     g->x_chunk = fk;
+    g->axis_split = split_env >= 0 ? split_env : (fs != 0 ? 1 : 0);
     return JXF_OK;
   }
   if (!enabled || g->n < (1LL << 18)) {
     TRY(heuristic_tune(g));
+    if (split_env >= 0) g->axis_split = split_env;
   } else {
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
-    int bc = 0, bk = 8;
+    int bc = 0, bk = 8, bs = 0;
     const int chunks[] = {8, 16, 32, 64};
-    for (int ci = 0; ci < (int)tma_configs().size(); ++ci) {
-      for (int ch : chunks) {
-        if (ch > g->d.nx && ch != 8) continue;
-        g->cfg = ci;
-        g->x_chunk = ch;
-        TRY(encode_maps(g));
-        Step3D p = base_params(g);
-        set_io(g, p, g->cur, 1 - g->cur);
-        p.blk_src_ptr = nullptr;
-        p.probe_out = nullptr;
-        p.step = 0;
-        p.err = g->d_err;
-        TRY(launch_step(g, ci, ch, p, g->cur, st));
-        CUDA_TRY(cudaEventRecord(e0, st));
-        const int reps = g->n >= (1LL << 25) ? 3 : 10;
-        for (int r = 0; r < reps; ++r) TRY(launch_step(g, ci, ch, p, g->cur, st));
-        CUDA_TRY(cudaEventRecord(e1, st));
-        CUDA_TRY(cudaEventSynchronize(e1));
-        float ms = 0;
-        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) {
-          best = ms;
-          bc = ci;
-          bk = ch;
+    const bool can_split = g->mode == MODE_CPML && !g->kappa;
+    for (int sp = 0; sp < 2; ++sp) {
+      if (sp == 1 && !can_split) continue;
+      if (split_env >= 0 && sp != split_env) continue;
+      for (int ci = 0; ci < (int)tma_configs().size(); ++ci) {
+        for (int ch : chunks) {
+          if (ch > g->d.nx && ch != 8) continue;
+          g->cfg = ci;
+          g->x_chunk = ch;
+          g->axis_split = sp;
+          TRY(encode_maps(g));
+          Step3D p = base_params(g);
+          set_io(g, p, g->cur, 1 - g->cur);
+          p.blk_src_ptr = nullptr;
+          p.probe_out = nullptr;
+          p.step = 0;
+          p.err = g->d_err;
+          TRY(launch_step(g, ci, ch, p, g->cur, st));
+          // trials of about 2 ms or more (small grids run many steps), best of two
+          const int reps = g->n >= (1LL << 25) ? 3 : (g->n >= (1LL << 21) ? 40 : 100);
+          float ms = 1e30f;
+          for (int trial = 0; trial < 2; ++trial) {
+            CUDA_TRY(cudaEventRecord(e0, st));
+            for (int r = 0; r < reps; ++r) TRY(launch_step(g, ci, ch, p, g->cur, st));
+            CUDA_TRY(cudaEventRecord(e1, st));
+            CUDA_TRY(cudaEventSynchronize(e1));
+            float t = 0;
+            CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+            ms = std::min(ms, t);
+          }
+          if (ms < best) {
+            best = ms;
+            bc = ci;
+            bk = ch;
+            bs = sp;
+          }
         }
       }
     }
@@ -668,13 +743,14 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
     cudaEventDestroy(e1);
     g->cfg = bc;
     g->x_chunk = bk;
+    g->axis_split = bs;
     g->maps_ok = false;  // maps hold the boxes of the last trial, not of the winner
     g->built_cfg = -1;
     // The trials wrote only the idle buffer set, which the next real step
     // overwrites before anything reads it.
   }
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = {g->cfg, g->x_chunk};
+  g_tune_cache[key] = std::make_tuple(g->cfg, g->x_chunk, g->axis_split);
   return JXF_OK;
 }
 
@@ -868,6 +944,7 @@ int jxf_grid3d_destroy(jxf_grid3d* g) {
   dfree(g->d_entries);
   dfree(g->d_blk_ptr);
   dfree(g->d_shell);
+  for (int a = 0; a < 3; ++a) dfree(g->d_shell_ax[a]);
   dfree(g->d_inner);
   dfree(g->adj_ck);
   dfree(g->adj_sg);
@@ -900,12 +977,14 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
     out->tile_z = out->tile_y = out->rows_per_thread = out->stages = out->x_chunk = 0;
   }
   out->device_bytes = g->bytes;
-  out->shell_blocks = g->n_shell;
+  out->shell_blocks = g->n_shell + g->n_shell_ax[0] + g->n_shell_ax[1] + g->n_shell_ax[2];
   out->interior_blocks = g->n_inner;
   if (g->path == JXF_PATH_GENERIC)
     out->kernels_per_step = 2 + (g->n_cells > 0 ? 1 : 0);
   else if (g->mode == MODE_CPML && g->split_cfg >= 0)
-    out->kernels_per_step = (g->n_shell > 0 ? 1 : 0) + (g->n_inner > 0 ? 1 : 0);
+    out->kernels_per_step = (g->n_shell > 0 ? 1 : 0) + (g->n_inner > 0 ? 1 : 0) +
+                            (g->n_shell_ax[0] > 0 ? 1 : 0) + (g->n_shell_ax[1] > 0 ? 1 : 0) +
+                            (g->n_shell_ax[2] > 0 ? 1 : 0);
   else
     out->kernels_per_step = 1;
   return JXF_OK;
@@ -922,6 +1001,12 @@ int jxf_grid3d_set_launch(jxf_grid3d* g, int32_t cfg, int32_t x_chunk) {
   g->x_chunk = x_chunk;
   g->maps_ok = false;
   g->built_cfg = -1;
+  return JXF_OK;
+}
+
+int jxf_grid3d_set_axis_split(jxf_grid3d* g, int32_t on) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  g->axis_split = on ? 1 : 0;
   return JXF_OK;
 }
 

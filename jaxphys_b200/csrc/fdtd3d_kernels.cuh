@@ -415,7 +415,33 @@ struct alignas(64) Maps3D {
 
 constexpr int round32(int v) { return (v + 31) / 32 * 32; }
 
-template <int TZ, int TY, int RY, int STAGES, bool CBARR, bool CPML>
+// psi arrays by differencing axis (x: HYX HZX EYX EZX, y: HXY HZY EXY EZY,
+// z: HXZ HYZ EXZ EYZ) and their slot in a block's psi ring when the block's
+// cells touch only the slab axes in the bit set `axes` (1 = x, 2 = y, 4 = z):
+// four slots per included axis; psi of excluded axes are never used.
+__host__ __device__ constexpr int psi_axis(int id) {
+  return (id == PSI_HYX || id == PSI_HZX || id == PSI_EYX || id == PSI_EZX)   ? 0
+         : (id == PSI_HXY || id == PSI_HZY || id == PSI_EXY || id == PSI_EZY) ? 1
+                                                                              : 2;
+}
+__host__ __device__ constexpr int psi_within(int id) {
+  return (id == PSI_HYX || id == PSI_HXY || id == PSI_HXZ)   ? 0
+         : (id == PSI_HZX || id == PSI_HZY || id == PSI_HYZ) ? 1
+         : (id == PSI_EYX || id == PSI_EXY || id == PSI_EXZ) ? 2
+                                                             : 3;
+}
+__host__ __device__ constexpr int psi_slot(int axes, int id) {
+  return ((axes >> psi_axis(id)) & 1) == 0
+             ? 0
+             : 4 * (((axes & 1) && psi_axis(id) > 0 ? 1 : 0) +
+                    ((axes & 2) && psi_axis(id) > 1 ? 1 : 0)) +
+                   psi_within(id);
+}
+__host__ __device__ constexpr int psi_count(int axes) {
+  return 4 * ((axes & 1 ? 1 : 0) + (axes & 2 ? 1 : 0) + (axes & 4 ? 1 : 0));
+}
+
+template <int TZ, int TY, int RY, int STAGES, bool CBARR, bool CPML, int AXES = 7>
 struct TmaLayout {
   static constexpr int TYT = TY / RY;
   static constexpr int NT = TZ * TYT;
@@ -432,7 +458,8 @@ struct TmaLayout {
   // CPML: psi of the planes in flight, per thread: 12 core values per row and
   // 4 halo values, in a ring of PSB buffers (prefetch distance PSB-1 planes).
   static constexpr int PSB = 2;
-  static constexpr int PSC_FLOATS = CPML ? PSB * PSI_COUNT * RY * NT : 0;
+  static constexpr int NPSI = psi_count(AXES);
+  static constexpr int PSC_FLOATS = CPML ? PSB * NPSI * RY * NT : 0;
   static constexpr int PSH_FLOATS = CPML ? PSB * 4 * (TZ + TY) : 0;
   static constexpr size_t SMEM_BYTES =
       128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + 3 * (size_t)HN_STRIDE +
@@ -469,11 +496,15 @@ __device__ __forceinline__ float pnext(bool on, float b, float c, float old, flo
   return on ? psi_next(b, old, c, d) : 0.0f;
 }
 
-template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA>
+// AXES (CPML only): the slab axes the block's cells may touch (1 = x, 2 = y,
+// 4 = z); the code and psi storage of the other axes compile away.  The host
+// launches single-axis variants for blocks that touch one slab axis only.
+template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA, int AXES = 7>
 __global__ void __launch_bounds__(TZ*(TY / RY))
     k3d_tma(const __grid_constant__ Step3D p, const __grid_constant__ Maps3D maps) {
   constexpr bool CPML = (MODE == MODE_CPML);
-  using L = TmaLayout<TZ, TY, RY, STAGES, CBARR, CPML>;
+  constexpr bool AX = (AXES & 1) != 0, AY = (AXES & 2) != 0, AZ = (AXES & 4) != 0;
+  using L = TmaLayout<TZ, TY, RY, STAGES, CBARR, CPML, AXES>;
   constexpr int TYT = L::TYT;
   constexpr int NT = L::NT;
   constexpr int NH = TZ + TY;  // halo threads
@@ -566,7 +597,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   float hyb = 1.f, hyc = 0.f, hyik = 1.f, hzb = 1.f, hzc = 0.f, hzik = 1.f;
   if (CPML) {
     const int km = (z < nz) ? slab_map(z, nz, p.pml.P[2]) : -1;
-    inz = km >= 0;
+    inz = AZ && km >= 0;
     if (z < nz) {
       zbh = __ldg(p.pml.tab[2][TAB_BH] + z);
       zch = __ldg(p.pml.tab[2][TAB_CH] + z);
@@ -582,7 +613,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       const int y = y0 + ty + r * TYT;
       const bool valid = (y < ny) && (z < nz);
       const int jm = (y < ny) ? slab_map(y, ny, p.pml.P[1]) : -1;
-      iny[r] = valid && jm >= 0;
+      iny[r] = AY && valid && jm >= 0;
       oy[r] = jm * nz + z;
       oz[r] = y * p.pml.L[2] + km;
       ox[r] = y * nz + z;
@@ -608,8 +639,8 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     if (yh >= 0) {
       const int jmh = slab_map(yh, ny, p.pml.P[1]);
       const int kmh = slab_map(zh, nz, p.pml.P[2]);
-      inyh = jmh >= 0;
-      inzh = kmh >= 0;
+      inyh = AY && jmh >= 0;
+      inzh = AZ && kmh >= 0;
       oyh = jmh * nz + zh;
       ozh = yh * p.pml.L[2] + kmh;
       oxh = yh * nz + zh;
@@ -630,7 +661,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       ybh[r] = ych[r] = ybe[r] = yce[r] = yikh[r] = yike[r] = 0.f;
     }
   }
-#define PSC(buf, id, r) PSc[(((buf) * PSI_COUNT + (id)) * RY + (r)) * NT + tid]
+#define PSC(buf, id, r) PSc[(((buf) * L::NPSI + psi_slot(AXES, (id))) * RY + (r)) * NT + tid]
 #define PSH(buf, k) PSh[((buf) * 4 + (k)) * NH + tid]
   // Prefetch psi_in of plane q into buffer `buf` (this thread's cells only).
   auto issue_psi = [&](int q, int buf) {
@@ -652,7 +683,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
         cp_async4(&PSC(buf, PSI_EXZ, r), p.pml.in[PSI_EXZ] + o);
         cp_async4(&PSC(buf, PSI_EYZ, r), p.pml.in[PSI_EYZ] + o);
       }
-      if (imq >= 0 && valid) {
+      if (AX && imq >= 0 && valid) {
         const int o = imq * SX + ox[r];
         cp_async4(&PSC(buf, PSI_HYX, r), p.pml.in[PSI_HYX] + o);
         cp_async4(&PSC(buf, PSI_HZX, r), p.pml.in[PSI_HZX] + o);
@@ -664,11 +695,11 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       if (inyh) cp_async4(&PSH(buf, 0), p.pml.in[PSI_HXY] + q * SY + oyh);
       if (inzh) cp_async4(&PSH(buf, 1), p.pml.in[PSI_HXZ] + q * SZ + ozh);
       if (tid < TZ) {  // row halo: Hz needs hzx, hzy
-        if (imq >= 0) cp_async4(&PSH(buf, 2), p.pml.in[PSI_HZX] + imq * SX + oxh);
+        if (AX && imq >= 0) cp_async4(&PSH(buf, 2), p.pml.in[PSI_HZX] + imq * SX + oxh);
         if (inyh) cp_async4(&PSH(buf, 3), p.pml.in[PSI_HZY] + q * SY + oyh);
       } else {  // column halo: Hy needs hyz, hyx
         if (inzh) cp_async4(&PSH(buf, 2), p.pml.in[PSI_HYZ] + q * SZ + ozh);
-        if (imq >= 0) cp_async4(&PSH(buf, 3), p.pml.in[PSI_HYX] + imq * SX + oxh);
+        if (AX && imq >= 0) cp_async4(&PSH(buf, 3), p.pml.in[PSI_HYX] + imq * SX + oxh);
       }
     }
     cp_async_commit();
@@ -727,7 +758,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     int imx = -1;
     float xbh = 1.f, xch = 0.f, xbe = 1.f, xce = 0.f, xikh = 1.f, xike = 1.f;
     if (CPML) {
-      imx = slab_map(x, nx, p.pml.P[0]);
+      imx = AX ? slab_map(x, nx, p.pml.P[0]) : -1;
       if (imx >= 0) {
         xbh = __ldg(p.pml.tab[0][TAB_BH] + x);
         xch = __ldg(p.pml.tab[0][TAB_CH] + x);

@@ -153,7 +153,8 @@ def test_cpml_tma_bitwise_generic_with_kappa_alpha(cuda):
 
 @pytest.mark.parametrize("cfg", range(N_TMA_CONFIGS))
 @pytest.mark.parametrize("chunk", [1, 3, 64])
-def test_every_launch_shape_bitwise(cuda, cfg, chunk):
+@pytest.mark.parametrize("split", [0, 1])
+def test_every_launch_shape_bitwise(cuda, cfg, chunk, split):
     """Every TMA tile shape and x-chunk (including 1-plane chunks, ragged tiles
     and sources on chunk seams) reproduces the generic kernel exactly."""
     from jaxphys_b200 import _native as nat
@@ -170,6 +171,7 @@ def test_every_launch_shape_bitwise(cuda, cfg, chunk):
             g.prepare(dt=rn.default_dt_3d(1.0))
             if path == "tma":
                 nat.check(nat.load().jxf_grid3d_set_launch(g._h, cfg, chunk), "set_launch")
+                nat.check(nat.load().jxf_grid3d_set_axis_split(g._h, split), "set_axis_split")
             tr = to_np(g.run(60))
             out.append(({k: to_np(g.field(k)) for k in COMPS}, tr))
     for k in COMPS:
