@@ -272,3 +272,48 @@ def test_band_destroy_refused_while_attached(cuda):
         m.close()
     g._release()
     m.close()
+
+
+def test_band_error_paths(cuda):
+    """Invalid uses fail with the library's error status, before any device work."""
+    import ctypes as C
+
+    import torch
+
+    from jaxphys_b200 import EMGrid3D
+    from jaxphys_b200 import _native as nat
+    from jaxphys_b200.em.batch import FDTDBatch
+    from jaxphys_b200.em.learned import LearnedBand
+    from jaxphys_b200.exceptions import ConfigurationError
+
+    lib = nat.load()
+    m = LearnedBand(seed=4)
+    # a band needs PEC walls
+    g = EMGrid3D((12, 12, 12), resolution=1.0, boundary="cpml", pml_layers=3, path="generic")
+    g.prepare()
+    b = FDTDBatch([g])
+    with pytest.raises(ConfigurationError):
+        b.set_band(m)
+    b.close()
+    # and every side >= 8
+    small = EMGrid3D((8, 8, 8), resolution=1.0, boundary="pec", path="generic")
+    small.prepare()
+    tiny_fields = [torch.zeros((7, 9, 9), device="cuda") for _ in range(6)]
+    ptrs = (C.c_void_p * 6)(*[t.data_ptr() for t in tiny_fields])
+    assert lib.jxf_band_collect(m._h, ptrs, 7, 9, 9, ptrs, 7, 9, 9, 0, 0, 0, None) == nat.ERR_INVALID
+    # a box outside the reference grid
+    f = [torch.zeros((10, 10, 10), device="cuda") for _ in range(6)]
+    fp = (C.c_void_p * 6)(*[t.data_ptr() for t in f])
+    assert lib.jxf_band_collect(m._h, fp, 10, 10, 10, fp, 10, 10, 10, 1, 0, 0, None) == nat.ERR_INVALID
+    # bad faces / shapes in eval
+    with pytest.raises(ConfigurationError):
+        m.eval(np.zeros((3, 54), np.float32), np.array([0, 6, 1], np.int32))
+    with pytest.raises(ConfigurationError):
+        m.eval(np.zeros((3, 50), np.float32), np.zeros(3, np.int32))
+    # parameters of the wrong shape
+    with pytest.raises(ConfigurationError):
+        m.params = np.zeros((6, 100), np.float32)
+    small._release()
+    g._release()
+    m.check()
+    m.close()
