@@ -104,10 +104,13 @@ int jxf_grid3d_set_axis_split(jxf_grid3d* g, int32_t on);
 /* Relative permittivity, replaces _build_epsilon_r (fdtd3d.py:132-137) and
  * the per-cell factor (dt_eps_dx / eps_r) of fdtd3d.py:299,336,345,354.
  * eps_r: nx*ny*nz float64 values in HOST memory (the library forms
- * dt/(eps0 dx)/eps_r in FP64 and rounds once), or NULL for vacuum. */
+ * dt/(eps0 dx)/eps_r in FP64 and rounds once), or NULL for vacuum.
+ * eps_r = +inf (extension) marks a perfect electric conductor cell: its
+ * factor is 0, so Ex, Ey and Ez of that cell keep their initial value (zero);
+ * zero, negative and NaN values are rejected. */
 int jxf_grid3d_set_eps_host(jxf_grid3d* g, const double* eps_r);
 /* Same from a DEVICE float32 array (e.g. a DLPack capsule's data pointer):
- * the division runs on the device in FP32. */
+ * the division runs on the device in FP32 (+inf gives 0, as above). */
 int jxf_grid3d_set_eps_device(jxf_grid3d* g, const float* eps_r, void* stream);
 
 /* Soft sources, replaces add_sources (fdtd3d.py:233-245): after the E update
@@ -262,8 +265,8 @@ int jxf_grid3d_check_finite(jxf_grid3d* g, void* stream);
 /* Allocation-free stepping.  No counterpart in the reference (its solver
  * allocates fresh JAX arrays on every call).  For callers that may not call
  * cudaMalloc: code living inside another framework's device memory pool (an
- * XLA custom call, for instance), work recorded into CUDA graphs, or hosts
- * that forbid allocation at run time.  Advances the caller's six float32
+ * XLA custom call, for instance, which must not take device memory behind
+ * the pool's back) or hosts that forbid allocation at run time.  Advances the caller's six float32
  * field buffers (device, C order (nx, ny, nz), Ex..Hz) by n_steps with the
  * reference's ABSORBING or PEC update and no sources, using a fixed device
  * scratch array inside the library (about 6 MB, held by every GPU that loads
@@ -323,6 +326,26 @@ int jxf_grid2d_set_field(jxf_grid2d* g, int32_t comp, const float* src,
  * frame (fdtd.py:359-386). */
 int jxf_grid2d_snapshot(jxf_grid2d* g, float* dst, void* stream);
 int jxf_grid2d_check_error(jxf_grid2d* g, void* stream);
+
+/* ------------------------------------------------------ field viewers */
+/* Extension, for the snapshot / animation writers (jaxphys_b200.viz) that
+ * replace the reference's matplotlib viewers (viz/fields.py:32-167) and read
+ * the fields where they live.  A slice is nu x nv FP32 samples at
+ * src[f*sf + c*su + r*sv] (DEVICE memory; strides in elements) for frames
+ * f < n_frames.
+ *
+ * *out (DEVICE float) = max |v| over all frames (stream-ordered). */
+int jxf_slice_absmax(const float* src, int64_t nu, int64_t nv, int64_t su, int64_t sv,
+                     int32_t n_frames, int64_t sf, float* out, void* stream);
+/* out (DEVICE, n_frames * nv * nu * 3 bytes): RGB images as the reference's
+ * imshow(data.T, origin="lower", vmin=-vmax, vmax=vmax): image row 0 is slice
+ * row nv-1, colour lut[k] (256 RGB entries, DEVICE) with
+ * k = floor((v/vmax + 1)/2 * 256) clamped to [0, 255].  vmax is read from
+ * vmax_dev when not NULL (e.g. jxf_slice_absmax's output), else the vmax
+ * argument; a zero vmax counts as 1 (viz/fields.py:63-65). */
+int jxf_slice_rgb(const float* src, int64_t nu, int64_t nv, int64_t su, int64_t sv,
+                  int32_t n_frames, int64_t sf, const float* vmax_dev, float vmax,
+                  const uint8_t* lut, uint8_t* out, void* stream);
 
 /* ------------------------------------------------------------------ misc */
 const char* jxf_last_error(void);

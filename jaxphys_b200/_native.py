@@ -137,6 +137,9 @@ SIGNATURES = {
     "jxf_batch3d_set_band": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_set_band": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_run_noalloc": (C.c_int, [C.POINTER(NoAllocDesc), C.POINTER(_vp), _vp, _i32, _vp]),
+    "jxf_slice_absmax": (C.c_int, [_vp, _i64, _i64, _i64, _i64, _i32, _i64, _vp, _vp]),
+    "jxf_slice_rgb": (C.c_int, [_vp, _i64, _i64, _i64, _i64, _i32, _i64, _vp, C.c_float, _vp,
+                                _vp, _vp]),
     "jxf_grid2d_create": (C.c_int, [C.POINTER(Grid2DDesc), C.POINTER(_vp)]),
     "jxf_grid2d_destroy": (C.c_int, [_vp]),
     "jxf_grid2d_set_sources": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),

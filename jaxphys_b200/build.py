@@ -21,7 +21,7 @@ OUT = HERE / "_lib" / "libjaxphys_fdtd.so"
 
 SOURCES = ["capi.cu"]
 HEADERS = ["fdtd_common.cuh", "fdtd3d_kernels.cuh", "fdtd3d_adjoint.cuh", "fdtd2d_kernels.cuh",
-           "tc_common.cuh", "learned_band.cuh"]
+           "tc_common.cuh", "learned_band.cuh", "viz_kernels.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

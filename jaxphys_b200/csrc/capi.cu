@@ -22,6 +22,7 @@
 #include "fdtd3d_adjoint.cuh"
 #include "fdtd3d_kernels.cuh"
 #include "learned_band.cuh"
+#include "viz_kernels.cuh"
 
 using namespace jxf;
 
@@ -770,6 +771,42 @@ const char* jxf_last_error(void) { return g_last_error.c_str(); }
 
 int jxf_version(void) { return 100; }
 
+// ---- field viewers (viz_kernels.cuh)
+static int slice_args(const float* src, int64_t nu, int64_t nv, int32_t n_frames) {
+  if (!src) return fail(JXF_ERR_INVALID, "null slice pointer");
+  if (nu <= 0 || nv <= 0 || n_frames <= 0)
+    return fail(JXF_ERR_INVALID, "empty slice (%lld x %lld, %d frames)", (long long)nu,
+                (long long)nv, n_frames);
+  return JXF_OK;
+}
+
+int jxf_slice_absmax(const float* src, int64_t nu, int64_t nv, int64_t su, int64_t sv,
+                     int32_t n_frames, int64_t sf, float* out, void* stream) {
+  TRY(slice_args(src, nu, nv, n_frames));
+  if (!out) return fail(JXF_ERR_INVALID, "null output");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long total = (long long)n_frames * nu * nv;
+  CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float), st));
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 8);
+  jxf::k_slice_absmax<<<blocks, 256, 0, st>>>(src, nu, nv, su, sv, sf, total, out);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
+int jxf_slice_rgb(const float* src, int64_t nu, int64_t nv, int64_t su, int64_t sv,
+                  int32_t n_frames, int64_t sf, const float* vmax_dev, float vmax,
+                  const uint8_t* lut, uint8_t* out, void* stream) {
+  TRY(slice_args(src, nu, nv, n_frames));
+  if (!lut || !out) return fail(JXF_ERR_INVALID, "null colour table or output");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long total = (long long)n_frames * nu * nv;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+  jxf::k_slice_rgb<<<blocks, 256, 0, st>>>(src, nu, nv, su, sv, sf, total, vmax_dev, vmax, lut,
+                                           out);
+  CUDA_TRY(cudaGetLastError());
+  return JXF_OK;
+}
+
 static int create3d(const jxf_grid3d_desc& d, int gnx, int gx0, int x_lo, int x_hi, bool slab,
                     jxf_grid3d** out);
 
@@ -1028,8 +1065,9 @@ int jxf_grid3d_set_eps_host(jxf_grid3d* g, const double* eps_r) {
   }
   std::vector<float> cb((size_t)g->n);
   for (long long i = 0; i < g->n; ++i) {
-    if (!(eps_r[i] > 0) || !std::isfinite(eps_r[i]))
-      return fail(JXF_ERR_INVALID, "eps_r must be finite and positive (cell %lld)", i);
+    // +inf marks a perfect electric conductor cell: Cb = 0 keeps its E at zero
+    if (!(eps_r[i] > 0) || std::isnan(eps_r[i]))
+      return fail(JXF_ERR_INVALID, "eps_r must be positive (or +inf) (cell %lld)", i);
     cb[i] = (float)(g->coef_e / eps_r[i]);  // fdtd3d.py:299 (dt_eps_dx / eps_r), FP64 then round
   }
   TRY(upload(&g->cb, cb, &g->bytes));
@@ -2696,8 +2734,8 @@ extern "C" int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_gra
 //
 // For callers that cannot call cudaMalloc: code that runs inside a memory
 // pool owned by another framework (for example an XLA custom call, which must
-// not grab device memory behind the pool's back), code recorded into a CUDA
-// graph, or hosts that forbid allocation once they are running.  The TMA step
+// not grab device memory behind the pool's back), or hosts that forbid
+// allocation once they are running.  The TMA step
 // kernel needs a second set of six field buffers to ping-pong into, plus the
 // damping tables and an error word; here they live in one fixed device array
 // that every GPU loading this library holds until the process exits.

@@ -1,7 +1,8 @@
-"""Electromagnetism: the FDTD Maxwell solvers (2D TM and 3D)."""
+"""Electromagnetism: the FDTD Maxwell solvers (2D TM and 3D) and waveguide mode ports."""
 
 from .fdtd import FDTD2D, EMGrid, PlaneWave, Wall
 from .fdtd3d import FDTD3D, CPMLSpec, DielectricRegion, EMGrid3D, PointSource3D
+from .waveguides import ModeSource3D, RectangularWaveguide, WaveguideMode
 
 __all__ = [
     "EMGrid",
@@ -13,4 +14,7 @@ __all__ = [
     "DielectricRegion",
     "CPMLSpec",
     "FDTD3D",
+    "RectangularWaveguide",
+    "WaveguideMode",
+    "ModeSource3D",
 ]

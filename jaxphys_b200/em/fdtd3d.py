@@ -164,6 +164,7 @@ class EMGrid3D:
         self._materials: list[DielectricRegion] = []
         self._eps_override: np.ndarray | None = None
         self._eps_device = None
+        self._conductor: np.ndarray | None = None
         self._probes: list[tuple[int, int, int, int]] = []
         self._cpml = cpml or CPMLSpec()
         self._device = device
@@ -188,7 +189,14 @@ class EMGrid3D:
         return (self._nx, self._ny, self._nz)
 
     def add_source(self, source: PointSource3D) -> None:
-        """Add a point source to the grid (fdtd3d.py:112-120)."""
+        """Add a point source to the grid (fdtd3d.py:112-120).
+
+        Extension: a ``waveguides.ModeSource3D`` (waveguide mode port) adds
+        its plane of point sources."""
+        if hasattr(source, "point_sources"):
+            for s in source.point_sources(self.size):
+                self.add_source(s)
+            return
         ix, iy, iz = source.position
         if not (0 <= ix < self._nx and 0 <= iy < self._ny and 0 <= iz < self._nz):
             raise ConfigurationError(
@@ -209,6 +217,22 @@ class EMGrid3D:
                 f"grid size {expected}"
             )
         self._materials.append(material)
+        self._dirty = True
+
+    def add_conductor(self, mask) -> None:
+        """Extension: perfect electric conductor cells (metal walls, waveguides).
+
+        ``mask`` is a boolean array of the grid shape; masked cells get an
+        infinite permittivity, so the E update factor there is zero and
+        Ex, Ey, Ez of those cells stay at zero (staircased metal).  Several
+        calls accumulate; the conductors apply over any permittivity set
+        by materials, ``set_permittivity`` or ``set_permittivity_device``.
+        """
+        m = np.asarray(_to_numpy(mask)).astype(bool)
+        if m.shape != self.size:
+            raise ConfigurationError(
+                f"Conductor mask shape {m.shape} doesn't match grid size {self.size}")
+        self._conductor = m.copy() if self._conductor is None else (self._conductor | m)
         self._dirty = True
 
     def set_permittivity(self, eps_r) -> None:
@@ -241,7 +265,7 @@ class EMGrid3D:
         t = eps_r.to(torch.float32).contiguous()
         self._eps_override = None
         self._eps_device = t
-        if self._h is not None and not self._dirty:
+        if self._h is not None and not self._dirty and self._conductor is None:
             nat.check(nat.load().jxf_grid3d_set_eps_device(self._h, t.data_ptr(),
                                                            nat.stream_handle()), "set_eps")
         else:
@@ -262,12 +286,15 @@ class EMGrid3D:
     def epsilon_r(self) -> np.ndarray:
         """Relative permittivity grid (fdtd3d.py:132-137, or the override)."""
         if self._eps_device is not None:
-            return self._eps_device.detach().cpu().numpy().astype(np.float64)
-        if self._eps_override is not None:
-            return self._eps_override
-        eps = np.ones(self.size)
-        for mat in self._materials:
-            eps = np.where(_to_numpy(mat.mask).astype(bool), mat.epsilon_r, eps)
+            eps = self._eps_device.detach().cpu().numpy().astype(np.float64)
+        elif self._eps_override is not None:
+            eps = self._eps_override
+        else:
+            eps = np.ones(self.size)
+            for mat in self._materials:
+                eps = np.where(_to_numpy(mat.mask).astype(bool), mat.epsilon_r, eps)
+        if self._conductor is not None:
+            eps = np.where(self._conductor, np.inf, eps)
         return eps
 
     def default_dt(self) -> float:
@@ -325,9 +352,15 @@ class EMGrid3D:
     def _upload_config(self) -> None:
         lib = nat.load()
         if self._eps_device is not None:
-            nat.check(lib.jxf_grid3d_set_eps_device(self._h, self._eps_device.data_ptr(),
+            t = self._eps_device
+            if self._conductor is not None:
+                import torch
+
+                t = t.masked_fill(torch.from_numpy(self._conductor).to(t.device), float("inf"))
+                self._eps_upload = t  # keep alive until the stream has read it
+            nat.check(lib.jxf_grid3d_set_eps_device(self._h, t.data_ptr(),
                                                     nat.stream_handle()), "set_eps")
-        elif self._eps_override is None and not self._materials:
+        elif self._eps_override is None and not self._materials and self._conductor is None:
             nat.check(lib.jxf_grid3d_set_eps_host(self._h, None), "set_eps")
         else:
             eps = np.ascontiguousarray(self.epsilon_r(), dtype=np.float64)

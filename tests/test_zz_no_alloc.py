@@ -1,8 +1,9 @@
 """The allocation-free entry point, jxf_grid3d_run_noalloc, through the C ABI.
 
 Some callers cannot call cudaMalloc: code that runs inside another
-framework's device memory pool (an XLA custom call, for instance), work that
-is recorded into CUDA graphs, or hosts that forbid allocation at run time.
+framework's device memory pool (an XLA custom call, for instance, which must
+not take device memory behind the pool's back) or hosts that forbid
+allocation at run time.
 For them the library keeps a fixed scratch array on every device and steps
 the caller's own field buffers with it.  This test checks that entry point
 against the regular handle-based one (jxf_grid3d_create / jxf_grid3d_step) on
