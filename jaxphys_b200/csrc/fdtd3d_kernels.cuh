@@ -472,16 +472,21 @@ struct TmaLayout {
   static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per block exceeds 227 KB");
 };
 
-// CPML component update written as a select: both the CPML and the plain
-// value are formed and the plain one is kept when neither axis of the
-// component is in its slab (the generic kernel branches on the same
-// condition, so the two paths produce identical bits).
+// CPML component update for a warp in which some lane is in a slab.  With
+// kappa = 1 the CPML form alone serves every lane: a lane outside both slabs
+// has p1 = p2 = 0 (pnext), and (d1 - d2) + 0 equals d1 - d2, so the result
+// equals the plain update h - a (d1 - d2) of the generic kernel (which
+// branches on the same condition) in value; only the sign of an exact zero
+// can differ, which no later +, -, * turns into a different number.  With
+// kappa > 1 the two values are formed and the plain one is selected (the
+// same bits as the generic kernel).
 template <bool KAPPA>
 __device__ __forceinline__ float h_sel(float h, float a, float d1, float d2, bool on1, bool on2,
                                        float p1, float p2, float ik1, float ik2) {
   const float u1 = KAPPA ? fmul(ik1, d1) : d1;
   const float u2 = KAPPA ? fmul(ik2, d2) : d2;
   const float c = fsub(h, fmul(a, fadd(fsub(u1, u2), fsub(p1, p2))));
+  if (!KAPPA) return c;
   return (on1 || on2) ? c : h_plain(h, a, d1, d2);
 }
 template <bool KAPPA>
@@ -490,6 +495,7 @@ __device__ __forceinline__ float e_sel(float e, float cb, float d1, float d2, bo
   const float u1 = KAPPA ? fmul(ik1, d1) : d1;
   const float u2 = KAPPA ? fmul(ik2, d2) : d2;
   const float c = fadd(e, fmul(cb, fadd(fsub(u1, u2), fsub(p1, p2))));
+  if (!KAPPA) return c;
   return (on1 || on2) ? c : e_plain(e, cb, d1, d2);
 }
 __device__ __forceinline__ float pnext(bool on, float b, float c, float old, float d) {

@@ -9,7 +9,9 @@ Tolerances (written per test):
   * probe traces over the whole run against FP64: relative L2 <= 1e-5;
   * against the FP32 oracle (the same roundings): relative L2 <= 1e-6;
   * TMA kernel against generic kernel: bit for bit (same operations, same
-    order).
+    order), compared with np.array_equal (kappa = 1 CPML warps apply the
+    CPML form with zero psi outside the slabs, equal in value to the plain
+    update; only the sign of an exact zero may differ).
 """
 
 import numpy as np
