@@ -568,6 +568,64 @@ bool range_clear(int lo, int hi, int n, int P) {
   return lo >= P && hi < n - P;
 }
 
+// JXF_SLAB_FIRST=0 keeps the row-major cell order in every CPML block.
+bool slab_first_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("JXF_SLAB_FIRST");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// JXF_BLOCK_ORDER=0 launches the CPML shell blocks in grid order instead of
+// heaviest first.
+bool heavy_first_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("JXF_BLOCK_ORDER");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+bool in_slab(int i, int n, int P) { return P < 0 || i < P || i >= n - P; }
+
+// Work of a CPML shell block in warp-planes: a warp holding a slab cell runs
+// the CPML update (counted 2), the others the plain one (1); every warp of a
+// plane inside the x slab runs CPML; the warm-up plane counts half.  All the
+// blocks of a small grid are resident at once, so the step lasts as long as
+// the most loaded SM: launching the blocks heaviest first spreads the heavy
+// ones over the SMs (the hardware hands out blocks in launch order).
+// Warps of a tile that run the CPML update on planes outside the x slab.
+int tile_cpml_warps(const jxf_grid3d* g, const TmaConfig& c, int z0, int y0, bool slab_first) {
+  const int ny = g->d.ny, nz = g->d.nz;
+  const int threads = c.threads, warps = (threads + 31) / 32;
+  std::vector<char> warp_cpml(warps, 0);
+  int n_cpml = 0;
+  for (int t = 0; t < threads; ++t) {
+    const int tx = t % c.tz, tyt = t / c.tz;
+    bool any = false;
+    for (int r = 0; r < c.ry; ++r) {
+      const int y = y0 + tyt + r * (c.ty / c.ry), z = z0 + tx;
+      if (y < ny && z < nz && (in_slab(y, ny, g->P[1]) || in_slab(z, nz, g->P[2]))) any = true;
+    }
+    if (any) {
+      ++n_cpml;
+      warp_cpml[t / 32] = 1;
+    }
+  }
+  return slab_first ? (n_cpml + 31) / 32 : (int)std::count(warp_cpml.begin(), warp_cpml.end(), 1);
+}
+
+double shell_block_cost(const jxf_grid3d* g, const TmaConfig& c, int cw, int xb, int xe) {
+  const int nx = g->d.nx, warps = (c.threads + 31) / 32;
+  double cost = 0.0;
+  for (int x = std::max(xb - 1, 0); x < xe; ++x) {
+    const double plane = in_slab(x, nx, g->P[0]) ? 2.0 * warps : 2.0 * cw + (warps - cw);
+    cost += x < xb ? 0.5 * plane : plane;
+  }
+  return cost;
+}
+
 int build_split(jxf_grid3d* g, int cfg, int chunk) {
   if (g->split_cfg == cfg && g->split_chunk == chunk && g->split_axes == g->axis_split)
     return JXF_OK;
@@ -575,6 +633,12 @@ int build_split(jxf_grid3d* g, int cfg, int chunk) {
   const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
   const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
   const int nch = (nx + chunk - 1) / chunk;
+  struct Blk {
+    double cost;
+    int tz, ty, word;
+  };
+  std::vector<Blk> shell_b, axl_b[3];
+  std::vector<int> tile_cw((size_t)ntz * nty, -1);  // filled on first use
   std::vector<int> shell, inner, axl[3];
   const bool axis_split = g->axis_split != 0;
   for (int ch = 0; ch < nch; ++ch)
@@ -587,13 +651,33 @@ int build_split(jxf_grid3d* g, int cfg, int chunk) {
         const bool cy = range_clear(y0 - 1, y0 + c.ty - 1, ny, g->P[1]);
         const bool cx = range_clear(xb - 1, xe - 1, nx, g->P[0]);
         const int touched = (cx ? 0 : 1) + (cy ? 0 : 1) + (cz ? 0 : 1);
-        std::vector<int>* v = &shell;
-        if (touched == 0) v = &inner;
-        else if (touched == 1 && !g->kappa && axis_split) v = &axl[!cx ? 0 : (!cy ? 1 : 2)];
-        v->push_back(tz);
-        v->push_back(ty);
-        v->push_back(ch);
+        if (touched == 0) {
+          inner.push_back(tz);
+          inner.push_back(ty);
+          inner.push_back(ch);
+          continue;
+        }
+        std::vector<Blk>* v = &shell_b;
+        if (touched == 1 && !g->kappa && axis_split) v = &axl_b[!cx ? 0 : (!cy ? 1 : 2)];
+        // blocks holding z-slab cells order them first (one row per thread)
+        const bool slab_first = !cz && c.ry == 1 && slab_first_enabled();
+        int& cw = tile_cw[(size_t)ty * ntz + tz];
+        if (cw < 0) cw = tile_cpml_warps(g, c, z0, y0, slab_first);
+        v->push_back({shell_block_cost(g, c, cw, xb, xe), tz, ty,
+                      ch | (slab_first ? BLK_SLAB_FIRST : 0)});
       }
+  auto flatten = [&](std::vector<Blk>& in, std::vector<int>& out) {
+    if (heavy_first_enabled())
+      std::stable_sort(in.begin(), in.end(),
+                       [](const Blk& u, const Blk& v) { return u.cost > v.cost; });
+    for (const Blk& b : in) {
+      out.push_back(b.tz);
+      out.push_back(b.ty);
+      out.push_back(b.word);
+    }
+  };
+  flatten(shell_b, shell);
+  for (int a = 0; a < 3; ++a) flatten(axl_b[a], axl[a]);
   TRY(upload(&g->d_shell, shell, &g->bytes));
   TRY(upload(&g->d_inner, inner, &g->bytes));
   for (int a = 0; a < 3; ++a) {

@@ -502,6 +502,60 @@ __device__ __forceinline__ float pnext(bool on, float b, float c, float old, flo
   return on ? psi_next(b, old, c, d) : 0.0f;
 }
 
+// Slab-first cell order of a CPML block (one row per thread): thread t takes
+// the t-th cell of the tile counted over the cells that lie in a y or z psi
+// slab first (y-slab rows whole, then the slab columns of the other rows,
+// row by row), then over the rest.  A tile whose 32-wide warps each hold a
+// few z-slab lanes (e.g. 11 of 32) would run every warp through the CPML
+// update; in this order the slab cells fill the first warps and the other
+// warps take the plain update.  The arithmetic of every cell is unchanged.
+// useY / useZ: the block's kernel handles that axis's slab; P < 0 stores
+// the whole axis.
+template <int TZ, int TY>
+__device__ __forceinline__ void slab_first_cell(int t, int z0, int y0, int nz, int ny, int P1,
+                                                int P2, bool useY, bool useZ, int& tx, int& ty) {
+  // CPML columns of a row outside the y slab: [0, c1) and [c2, cv)
+  const int cv = min(TZ, nz - z0);
+  int c1 = 0, c2 = cv;
+  if (useZ) {
+    if (P2 < 0) {
+      c1 = cv;
+    } else {
+      c1 = min(max(P2 - z0, 0), cv);
+      c2 = max(c1, min(max(nz - P2 - z0, 0), cv));
+    }
+  }
+  const int ncz = c1 + (cv - c2);  // CPML cells of such a row
+  const int gap = c2 - c1;         // its other cells: [c1, c2) then [cv, TZ)
+  int k = t, nc = 0;
+#pragma unroll
+  for (int i = 0; i < TY; ++i) {
+    const int y = y0 + i;
+    const bool yin = useY && y < ny && (P1 < 0 || y < P1 || y >= ny - P1);
+    nc += yin ? TZ : (y < ny ? ncz : 0);
+  }
+  const bool first = t < nc;
+  if (!first) k = t - nc;
+  tx = 0;
+  ty = TY - 1;
+  bool done = false;
+#pragma unroll
+  for (int i = 0; i < TY; ++i) {
+    const int y = y0 + i;
+    const bool valid = y < ny;
+    const bool yin = useY && valid && (P1 < 0 || y < P1 || y >= ny - P1);
+    const int cnt = first ? (yin ? TZ : (valid ? ncz : 0)) : (yin ? 0 : (valid ? TZ - ncz : TZ));
+    if (!done && k < cnt) {
+      ty = i;
+      if (yin || !valid) tx = k;
+      else if (first) tx = k < c1 ? k : c2 + (k - c1);
+      else tx = k < gap ? c1 + k : cv + (k - gap);
+      done = true;
+    }
+    if (!done) k -= cnt;
+  }
+}
+
 // AXES (CPML only): the slab axes the block's cells may touch (1 = x, 2 = y,
 // 4 = z); the code and psi storage of the other axes compile away.  The host
 // launches single-axis variants for blocks that touch one slab axis only.
@@ -525,16 +579,21 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
 
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int tid = threadIdx.x;
-  const int tx = tid % TZ;
-  const int ty = tid / TZ;
   int tzi = blockIdx.x, tyi = blockIdx.y, ci = blockIdx.z;
+  bool slab_first = false;
   if (p.blk_list != nullptr) {
     tzi = p.blk_list[3 * blockIdx.x];
     tyi = p.blk_list[3 * blockIdx.x + 1];
-    ci = p.blk_list[3 * blockIdx.x + 2];
+    const int v = p.blk_list[3 * blockIdx.x + 2];
+    ci = v & BLK_CHUNK_MASK;
+    slab_first = (v & BLK_SLAB_FIRST) != 0;
   }
   const int z0 = tzi * TZ;
   const int y0 = tyi * TY;
+  int tx = tid % TZ;
+  int ty = tid / TZ;
+  if (CPML && RY == 1 && slab_first)
+    slab_first_cell<TZ, TY>(tid, z0, y0, nz, ny, p.pml.P[1], p.pml.P[2], AY, AZ, tx, ty);
   const int xb = ci * p.x_chunk;
   const int xe = min(xb + p.x_chunk, nx);
   const int qs = xb > 0 ? xb - 1 : 0;  // first plane staged

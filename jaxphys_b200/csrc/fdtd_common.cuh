@@ -13,6 +13,10 @@
 
 namespace jxf {
 
+// chunk word of a blk_list entry: x chunk index | flags
+constexpr int BLK_CHUNK_MASK = 0x3fffffff;
+constexpr int BLK_SLAB_FIRST = 0x40000000;
+
 enum Mode : int { MODE_ABSORB = 0, MODE_PERIODIC = 1, MODE_PEC = 2, MODE_CPML = 3 };
 
 // psi array order (component of the field, then differencing axis)
@@ -120,7 +124,8 @@ struct Step3D {
   int ntiles_y, ntiles_z;
   // Optional compact list of blocks (tile_z, tile_y, chunk) triples; nullptr
   // = the launch grid itself.  Used to run the shell and the interior of a
-  // CPML grid as two launches with different kernels.
+  // CPML grid as separate launches with different kernels.  The chunk word
+  // carries BLK_SLAB_FIRST for blocks that order their cells slab-first.
   const int* blk_list;
   int pdl;  // PDL_* bits
   // x-slab of a decomposed grid (generic kernels): local planes [x_lo, x_hi)
