@@ -784,7 +784,9 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
     CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
     int bc = 0, bk = 8, bs = 0;
-    const int chunks[] = {8, 16, 32, 64};
+    // short chunks give small grids more blocks (64^3: 2 planes per block is
+    // fastest), long ones cut the warm-up plane share on large grids
+    const int chunks[] = {2, 4, 8, 16, 32, 64};
     const bool can_split = g->mode == MODE_CPML && !g->kappa;
     for (int sp = 0; sp < 2; ++sp) {
       if (sp == 1 && !can_split) continue;

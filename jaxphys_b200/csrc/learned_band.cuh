@@ -185,6 +185,14 @@ __device__ __forceinline__ float gather(const GridRef& g, int cell, int face, fl
   return sqrtf(ss * (1.0f / kIn) + 1e-30f);
 }
 
+// This thread waits for `bar`; true if the wait gave up (recorded in err).
+__device__ __forceinline__ bool wait_one(uint64_t* bar, uint32_t phase, unsigned long long ns,
+                                         int* err, int where) {
+  const bool ok = mbar_wait_bounded(bar, phase, ns);
+  if (!ok) report_error(err, ERR_TIMEOUT_BASE | 0x100 | where, blockIdx.x, blockIdx.y, threadIdx.x);
+  return !ok;
+}
+
 // All threads wait for `bar`; false (for every thread) if any timed out.
 __device__ __forceinline__ bool wait_all(uint64_t* bar, uint32_t phase, unsigned long long ns,
                                         int* err, int where) {
@@ -247,9 +255,12 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
   const uint32_t lane_base = tc::taddr(tm, (tid >> 5) * 32, 0);
   const uint32_t sA = smem_u32(bufA), sW = smem_u32(bufW);
   constexpr uint32_t id64 = tc::idesc_bf16(128, 64), id16 = tc::idesc_bf16(128, 16);
+  // Every thread waits on the MMA barrier itself (so no CTA barrier follows
+  // an MMA); a wait that gave up is voted at the next CTA barrier, before
+  // the next MMA is issued.  Three CTA barriers per tile.
   uint32_t phase = 0;
   int cur_face = -1;
-  bool ok = true;
+  bool ok = true, timed = false;
   for (int t = t0; t < t1 && ok; ++t) {
     const int face = p.tile_face[t];
     if (face != cur_face) {
@@ -283,7 +294,10 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
     put_row_f32(bufA, tid, v, kKH);
     fence_proxy_async();
     tc::fence_before_sync();
-    __syncthreads();
+    if (__syncthreads_or(timed)) {
+      ok = false;
+      break;
+    }
     // layer 1: Z1 = [X 1] [W1 b1]^T
     if (tid == 0) {
       tc::fence_after_sync();
@@ -292,9 +306,8 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
         tc::mma(tm, tc::img_desc(sA, kKH, kk), tc::img_desc(sW + kImgW1, 64, kk), id64, kk);
       tc::commit(bar);
     }
-    ok = wait_all(bar, phase, p.wait_ns, p.err, 1);
+    timed |= wait_one(bar, phase, p.wait_ns, p.err, 1);
     phase ^= 1;
-    if (!ok) break;
     tc::fence_after_sync();
     uint32_t g[32];
     {
@@ -309,7 +322,10 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
     put_row_packed(bufA, tid, g, kKH);
     fence_proxy_async();
     tc::fence_before_sync();
-    __syncthreads();
+    if (__syncthreads_or(timed)) {
+      ok = false;
+      break;
+    }
     // layer 2: Z2 = [G1 1] [W2 b2]^T
     if (tid == 0) {
       tc::fence_after_sync();
@@ -318,9 +334,8 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
         tc::mma(tm, tc::img_desc(sA, kKH, kk), tc::img_desc(sW + kImgW2, kKH, kk), id64, kk);
       tc::commit(bar);
     }
-    ok = wait_all(bar, phase, p.wait_ns, p.err, 2);
+    timed |= wait_one(bar, phase, p.wait_ns, p.err, 2);
     phase ^= 1;
-    if (!ok) break;
     tc::fence_after_sync();
     {
       float z[32];
@@ -334,7 +349,10 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
     put_row_packed(bufA, tid, g, kKH);
     fence_proxy_async();
     tc::fence_before_sync();
-    __syncthreads();
+    if (__syncthreads_or(timed)) {
+      ok = false;
+      break;
+    }
     // layer 3: O = [G2 1] [W3 b3]^T  (columns 0..15)
     if (tid == 0) {
       tc::fence_after_sync();
@@ -343,21 +361,22 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
         tc::mma(tm, tc::img_desc(sA, kKH, kk), tc::img_desc(sW + kImgW3, kKH, kk), id16, kk);
       tc::commit(bar);
     }
-    ok = wait_all(bar, phase, p.wait_ns, p.err, 3);
+    timed |= wait_one(bar, phase, p.wait_ns, p.err, 3);
     phase ^= 1;
-    if (!ok) break;
     tc::fence_after_sync();
+    // Every thread saw the MMA complete before it reads O, so the next
+    // tile's image and weight writes cannot race the MMAs of this one; the
+    // next MMA is issued after the next CTA barrier, when every thread has
+    // read its rows of O.
     tc::ld16(lane_base, v);
-    if (cg.x >= 0) {
+    if (cg.x >= 0 && !timed) {
       float* d = p.delta + (size_t)i * kOut;
 #pragma unroll
       for (int o = 0; o < kOut; ++o) d[o] = s * v[o];
     }
-    tc::fence_before_sync();
-    __syncthreads();
   }
   tc::fence_before_sync();
-  __syncthreads();
+  if (__syncthreads_or(timed)) ok = false;
   if (!ok) {
     // the commit that timed out may still be outstanding: give it one more bounded wait
     mbar_wait_bounded(bar, phase ^ 1, p.wait_ns);
