@@ -57,7 +57,7 @@ BAND_WEIGHTS = ROOT / "jaxphys_b200" / "em" / "band_weights.npz"
 # DRAM bytes per leapfrog step (CPML shell launch + interior launch) from the
 # ncu capture of the same workload and launch shape
 # (profiles/k3d_tma_cpml_128cubed_bench_c2.md); None where not captured.
-NCU_TRAFFIC = {"c2": 130.7e6, "c1": None, "c3": None}
+NCU_TRAFFIC = {"c2": 129.8e6, "c1": None, "c3": None}
 
 
 def make_inputs(name: str, seed: int = 0):
