@@ -131,7 +131,12 @@ __device__ __forceinline__ void init_hidden_tail(unsigned char* img, int tid, in
 }
 
 // Raw stencil of an outer cell (v[54], H scaled by eta0); returns s.
-__device__ __forceinline__ float gather(const GridRef& g, int cell, int face, float* v) {
+// Every load is issued before any value is used: positions outside the grid
+// along the tangent are loaded from the clamped (in-grid) neighbour and then
+// replaced by zero, so no load sits behind a branch and a thread keeps all
+// 54 (x, y faces) or 18 (z faces) loads in flight at once.
+__device__ __forceinline__ float gather(const GridRef& gref, int cell, int face, float* v) {
+  const GridRef g = gref;
   const int a = face >> 1, side = face & 1;
   float ss = 0.0f;
   if (a == 2 && (g.nz & 3) == 0) {
@@ -139,16 +144,24 @@ __device__ __forceinline__ float gather(const GridRef& g, int cell, int face, fl
     const long long row = (long long)cell - (side ? g.nz - 1 : 0) + (side ? g.nz - 4 : 0);
     const int x = cell / (g.nz * g.ny);
     const long long sx = (long long)g.ny * g.nz;
+    float4 q[3][6];
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+      const int xw = min(max(x + w - 1, 0), g.nx - 1);
+#pragma unroll
+      for (int comp = 0; comp < 6; ++comp)
+        q[w][comp] = __ldg(reinterpret_cast<const float4*>(g.f[comp] + row + (xw - x) * sx));
+    }
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
       const bool in = x + w - 1 >= 0 && x + w - 1 < g.nx;
 #pragma unroll
       for (int comp = 0; comp < 6; ++comp) {
-        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (in) q = __ldg(reinterpret_cast<const float4*>(g.f[comp] + row + (w - 1) * sx));
         const float sc = comp >= 3 ? kEta0 : 1.0f;
-        const float l0 = (side ? q.w : q.x) * sc, l1 = (side ? q.z : q.y) * sc,
-                    l2 = (side ? q.y : q.z) * sc;
+        const float4 r = q[w][comp];
+        const float l0 = in ? (side ? r.w : r.x) * sc : 0.0f;
+        const float l1 = in ? (side ? r.z : r.y) * sc : 0.0f;
+        const float l2 = in ? (side ? r.y : r.z) * sc : 0.0f;
         v[comp * 9 + 0 * 3 + w] = l0;
         v[comp * 9 + 1 * 3 + w] = l1;
         v[comp * 9 + 2 * 3 + w] = l2;
@@ -166,16 +179,26 @@ __device__ __forceinline__ float gather(const GridRef& g, int cell, int face, fl
   const long long st = t1 == 0 ? sx : (t1 == 1 ? (long long)g.nz : 1ll);
   const int ct = t1 == 0 ? x : (t1 == 1 ? y : z);
   const int nt = t1 == 0 ? g.nx : (t1 == 1 ? g.ny : g.nz);
+  float raw[3][3][6];
 #pragma unroll
   for (int l = 0; l < 3; ++l) {
     const long long dn = side ? -l * sa : l * sa;
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
+      const int cw = min(max(ct + w - 1, 0), nt - 1);
+      const long long idx = (long long)cell + dn + (long long)(cw - ct) * st;
+#pragma unroll
+      for (int comp = 0; comp < 6; ++comp) raw[l][w][comp] = __ldg(g.f[comp] + idx);
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
       const bool in = ct + w - 1 >= 0 && ct + w - 1 < nt;
-      const long long idx = (long long)cell + dn + (long long)(w - 1) * st;
 #pragma unroll
       for (int comp = 0; comp < 6; ++comp) {
-        float val = in ? __ldg(g.f[comp] + idx) : 0.0f;
+        float val = in ? raw[l][w][comp] : 0.0f;
         if (comp >= 3) val *= kEta0;
         v[comp * 9 + l * 3 + w] = val;
         ss = fmaf(val, val, ss);
@@ -261,8 +284,11 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
   uint32_t phase = 0;
   int cur_face = -1;
   bool ok = true, timed = false;
+  int2 cg_next = p.cells[t0 * kTile + tid];  // (cell, grid) of the next tile, loaded a tile early
   for (int t = t0; t < t1 && ok; ++t) {
     const int face = p.tile_face[t];
+    const int2 cg = cg_next;
+    if (t + 1 < t1) cg_next = p.cells[(t + 1) * kTile + tid];
     if (face != cur_face) {
       const uint4* src = reinterpret_cast<const uint4*>(p.wimg + (size_t)face * kImgBytes);
       uint4* dst = reinterpret_cast<uint4*>(bufW);
@@ -270,7 +296,6 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
       cur_face = face;
     }
     const int i = t * kTile + tid;
-    const int2 cg = p.cells[i];
     float v[kInP];
     float s = 0.0f;
     if (cg.x >= 0) {
