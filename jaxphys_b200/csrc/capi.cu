@@ -2025,6 +2025,17 @@ int band_setup_attrs() {
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, band::kInfSmem));
     CUDA_TRY(cudaFuncSetAttribute(band::k_band_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   band::kTrSmem));
+    // The carveout is only a hint, and without one the driver may configure
+    // less shared memory than the CTAs per SM the grid is sized for (the
+    // launch then runs in several waves): ask for the largest split.
+    CUDA_TRY(cudaFuncSetAttribute(band::k_band_infer<band::SRC_GRIDS>,
+                                  cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    CUDA_TRY(cudaFuncSetAttribute(band::k_band_infer<band::SRC_ROWS>,
+                                  cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    CUDA_TRY(cudaFuncSetAttribute(band::k_band_train, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
     done = 1;
   }
   return JXF_OK;
@@ -2123,6 +2134,8 @@ int band_ctas(int n_tiles, int device) {
   const int by_smem = smem_sm / (band::kInfSmem + 1024);
   const int by_regs = regs_sm / (regs * 128);
   const int by_tmem = 512 / band::kInfTmemCols;
+  // (the runtime's occupancy query reports 1 block per SM for this kernel,
+  // while 5 run side by side: measured, so the count comes from the limits)
   const int occ = std::max(1, std::min(std::min(by_smem, by_regs), by_tmem));
   return std::max(1, std::min(n_tiles, sms * occ));
 }

@@ -409,18 +409,23 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
   if (tid < 32) tc::tmem_dealloc(tm, kInfTmemCols);
 }
 
-// X_c += delta (H rescaled); padding entries skipped.
+// X_c += delta (H rescaled); padding entries skipped.  The grid record is
+// copied into registers once (through a reference into global memory every
+// store would force the field pointers to be reloaded), and all six fields
+// are read before any is written, so a thread's loads are in flight together.
 __global__ void k_band_apply(const GridRef* grids, const int2* cells, int n, const float* delta) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int2 cg = cells[i];
   if (cg.x < 0) return;
-  const GridRef& g = grids[cg.y];
+  const GridRef g = grids[cg.y];
+  float d[kOut], f[6];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    const float d = delta[(size_t)i * kOut + c];
-    g.f[c][cg.x] += c >= 3 ? d * (1.0f / kEta0) : d;
-  }
+  for (int c = 0; c < 6; ++c) d[c] = delta[(size_t)i * kOut + c];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) f[c] = g.f[c][cg.x];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) g.f[c][cg.x] = __fadd_rn(f[c], c >= 3 ? d[c] * (1.0f / kEta0) : d[c]);
 }
 
 // ---------------------------------------------------------------------------
