@@ -462,7 +462,7 @@ struct TmaLayout {
   static constexpr int PSC_FLOATS = CPML ? PSB * NPSI * RY * NT : 0;
   static constexpr int PSH_FLOATS = CPML ? PSB * 4 * (TZ + TY) : 0;
   static constexpr size_t SMEM_BYTES =
-      128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + 3 * (size_t)HN_STRIDE +
+      128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + 6 * (size_t)HN_STRIDE +
                              PSC_FLOATS + PSH_FLOATS);
   static_assert(TY % RY == 0, "rows per thread must divide the tile height");
   static_assert(TZ % 4 == 0, "tile width must keep TMA x coordinates 16-byte aligned");
@@ -573,8 +573,13 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
   float* stages = reinterpret_cast<float*>(smem_raw + 128);
-  float* Hn = stages + STAGES * L::STAGE_FLOATS;
-  float* PSc = Hn + 3 * L::HN_STRIDE;
+  // H of the current plane (tile + halo row / column), double-buffered by
+  // plane parity: plane l writes buffer l & 1 in its H phase and reads it in
+  // its E phase; plane l + 2 overwrites it only after every thread has passed
+  // plane l + 1's barrier, i.e. finished plane l's E phase.  So a plane needs
+  // one CTA barrier (between its H and E phases), not two.
+  float* HnB = stages + STAGES * L::STAGE_FLOATS;
+  float* PSc = HnB + 6 * L::HN_STRIDE;
   float* PSh = PSc + L::PSC_FLOATS;
 
   const int nx = p.nx, ny = p.ny, nz = p.nz;
@@ -815,6 +820,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     const float* En = stages + ((l + 1) % STAGES) * L::STAGE_FLOATS;
     const float* Hs = Es + 3 * L::E_STRIDE;
     const float* CBs = Hs + 3 * L::H_STRIDE;
+    float* const Hn = HnB + (l & 1) * 3 * L::HN_STRIDE;
 #define E_AT(c, yy, zc) Es[(c) * L::E_STRIDE + (yy) * EW + (zc)]
 #define EN_AT(c, yy, zc) En[(c) * L::E_STRIDE + (yy) * EW + (zc)]
 #define H_AT(c, yy, zc) Hs[(c) * L::H_STRIDE + (yy) * HW + (zc)]
@@ -838,11 +844,14 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     const bool inx = imx >= 0;
 
     // ---------------- H^{n+1/2} on the tile (registers + Hn) ----------------
-    float exr[RY], eyr[RY], ezr[RY], hxr[RY], hyr[RY], hzr[RY];
+    float exr[RY], eyr[RY], ezr[RY], hxr[RY], hyr[RY], hzr[RY], cbr[RY];
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       const int yl = ty + r * TYT;
       const int y = y0 + yl;
+      // Cb is read here, with the rest of the stage: after this plane's
+      // barrier the stage slot is refilled
+      cbr[r] = CBARR ? CBs[yl * TZ + tx] : p.cb_const;
       const int yy = yl + 1;
       const bool valid = (y < ny) && (z < nz);
       const bool own = !warm && valid;
@@ -959,6 +968,13 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       aborted = true;
       break;
     }
+    // Every thread is done with stage `slot` (this H phase and the previous
+    // plane's read it; Cb came along above): refill it now.
+    consumed = l + 1;
+    if (issued < nload && issued < consumed + STAGES) {
+      if (tid == 0) issue(issued);
+      ++issued;
+    }
 
     if (!warm) {
       // ---------------- E^{n+1} on the tile ----------------
@@ -971,7 +987,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
         const bool own = (y < ny) && (z < nz);
         float ex = exr[r], ey = eyr[r], ez = ezr[r];
         const float hxc = hxr[r], hyc = hyr[r], hzc = hzr[r];
-        const float cb = CBARR ? CBs[yl * TZ + tx] : p.cb_const;
+        const float cb = cbr[r];
         const bool ux = y >= 1 && z >= 1, uy = x >= 1 && z >= 1, uz = x >= 1 && y >= 1;
         const float dyHz = fsub(hzc, HN_AT(2, yy - 1, zn)), dzHy = fsub(hyc, HN_AT(1, yy, zn - 1));
         const float dzHx = fsub(hxc, HN_AT(0, yy, zn - 1)), dxHz = fsub(hzc, hz_prev[r]);
@@ -1059,12 +1075,6 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
 #undef EN_AT
 #undef H_AT
 #undef HN_AT
-    __syncthreads();  // Hn and stage `slot` are free again
-    consumed = l + 1;
-    if (issued < nload && issued < consumed + STAGES) {
-      if (tid == 0) issue(issued);
-      ++issued;
-    }
   }
 #undef PSC
 #undef PSH
