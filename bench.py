@@ -57,7 +57,7 @@ BAND_WEIGHTS = ROOT / "jaxphys_b200" / "em" / "band_weights.npz"
 # DRAM bytes per leapfrog step (CPML shell launch + interior launch) from the
 # ncu capture of the same workload and launch shape
 # (profiles/k3d_tma_cpml_128cubed_bench_c2.md); None where not captured.
-NCU_TRAFFIC = {"c2": 129.8e6, "c1": None, "c3": None}
+NCU_TRAFFIC = {"c2": 81.7e6, "c1": None, "c3": None}
 
 
 def make_inputs(name: str, seed: int = 0):
@@ -309,13 +309,15 @@ def run_ours(args, world, rank, local, pg):
                    "path": "tma" if info["path"] == 2 else "generic",
                    "tile": [info["tile_z"], info["tile_y"], info["rows_per_thread"],
                             info["stages"], info["x_chunk"]],
+                   "launch": {"tma_config": info["tma_config"], "x_chunk": info["x_chunk"],
+                              "axis_split": info["axis_split"]},
                    "parallelism": f"independent grid per GPU x{world}"},
         "e2e": {"value": round(e2e_value, 3), "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": peak_kind, "bytes_per_cell_update": round(b_cell, 2),
-                     "kernel": "k3d_tma step (CPML shell launch + plain interior launch)",
+                     "kernel": "k3d_tma step (every launch of one leapfrog step)",
                      "ms_per_leapfrog_step": round(per_launch_ms, 5)},
         "gpu_launches": (nsteps * g.kernels_per_step() + 1) * args.steps,
         "clocks": clocks,

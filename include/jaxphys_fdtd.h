@@ -84,6 +84,8 @@ typedef struct {
   int64_t device_bytes;       /* device memory held by the handle         */
   int32_t kernels_per_step;   /* step kernels launched per leapfrog step  */
   int32_t shell_blocks, interior_blocks;  /* CPML region split (TMA path) */
+  int32_t tma_config;         /* launch-shape registry entry (TMA path)   */
+  int32_t axis_split;         /* single-axis CPML shell split on (1)/off  */
 } jxf_grid3d_info;
 
 int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out);

@@ -54,6 +54,7 @@ class Grid3DInfo(C.Structure):
         ("device_bytes", C.c_int64),
         ("kernels_per_step", C.c_int32),
         ("shell_blocks", C.c_int32), ("interior_blocks", C.c_int32),
+        ("tma_config", C.c_int32), ("axis_split", C.c_int32),
     ]
 
 

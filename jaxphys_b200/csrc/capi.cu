@@ -527,6 +527,10 @@ int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStr
     size_t& have = done[{k, g->d.device}];
     if (have < smem) {
       CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      // the carveout is a hint the driver may undercut (down to one block per
+      // SM for the large-tile shapes): ask for the largest shared split
+      CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared));
       have = smem;
     }
   }
@@ -1102,6 +1106,8 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
   out->device_bytes = g->bytes;
   out->shell_blocks = g->n_shell + g->n_shell_ax[0] + g->n_shell_ax[1] + g->n_shell_ax[2];
   out->interior_blocks = g->n_inner;
+  out->tma_config = g->path == JXF_PATH_TMA ? g->cfg : -1;
+  out->axis_split = g->axis_split;
   if (g->path == JXF_PATH_GENERIC)
     out->kernels_per_step = 2 + (g->n_cells > 0 ? 1 : 0);
   else if (g->mode == MODE_CPML && g->split_cfg >= 0)
