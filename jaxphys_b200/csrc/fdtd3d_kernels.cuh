@@ -455,6 +455,10 @@ struct TmaLayout {
   static constexpr uint32_t STAGE_TX =
       (uint32_t)(3 * EH * EW + 3 * HH * HW + (CBARR ? TY * TZ : 0)) * 4u;
   static constexpr int HN_STRIDE = round32(NH * NW);
+  // new-H plane buffers: two (one CTA barrier per plane) for one row per
+  // thread; one (two barriers) for several rows per thread, whose larger
+  // tiles would otherwise lose a resident block per SM to shared memory
+  static constexpr int HNB = RY == 1 ? 2 : 1;
   // CPML: psi of the planes in flight, per thread: 12 core values per row and
   // 4 halo values, in a ring of PSB buffers (prefetch distance PSB-1 planes).
   static constexpr int PSB = 2;
@@ -462,7 +466,7 @@ struct TmaLayout {
   static constexpr int PSC_FLOATS = CPML ? PSB * NPSI * RY * NT : 0;
   static constexpr int PSH_FLOATS = CPML ? PSB * 4 * (TZ + TY) : 0;
   static constexpr size_t SMEM_BYTES =
-      128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + 6 * (size_t)HN_STRIDE +
+      128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + 3 * HNB * (size_t)HN_STRIDE +
                              PSC_FLOATS + PSH_FLOATS);
   static_assert(TY % RY == 0, "rows per thread must divide the tile height");
   static_assert(TZ % 4 == 0, "tile width must keep TMA x coordinates 16-byte aligned");
@@ -573,13 +577,15 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
   float* stages = reinterpret_cast<float*>(smem_raw + 128);
-  // H of the current plane (tile + halo row / column), double-buffered by
-  // plane parity: plane l writes buffer l & 1 in its H phase and reads it in
-  // its E phase; plane l + 2 overwrites it only after every thread has passed
-  // plane l + 1's barrier, i.e. finished plane l's E phase.  So a plane needs
-  // one CTA barrier (between its H and E phases), not two.
+  // H of the current plane (tile + halo row / column).  With two buffers
+  // (L::HNB == 2) they alternate by plane parity: plane l writes buffer l & 1
+  // in its H phase and reads it in its E phase; plane l + 2 overwrites it only
+  // after every thread has passed plane l + 1's barrier, i.e. finished plane
+  // l's E phase, so a plane needs one CTA barrier (between its H and E
+  // phases).  With one buffer a second barrier ends each plane.
+  constexpr bool ONE_BARRIER = L::HNB == 2;
   float* HnB = stages + STAGES * L::STAGE_FLOATS;
-  float* PSc = HnB + 6 * L::HN_STRIDE;
+  float* PSc = HnB + 3 * L::HNB * L::HN_STRIDE;
   float* PSh = PSc + L::PSC_FLOATS;
 
   const int nx = p.nx, ny = p.ny, nz = p.nz;
@@ -820,7 +826,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     const float* En = stages + ((l + 1) % STAGES) * L::STAGE_FLOATS;
     const float* Hs = Es + 3 * L::E_STRIDE;
     const float* CBs = Hs + 3 * L::H_STRIDE;
-    float* const Hn = HnB + (l & 1) * 3 * L::HN_STRIDE;
+    float* const Hn = HnB + (ONE_BARRIER ? (l & 1) : 0) * 3 * L::HN_STRIDE;
 #define E_AT(c, yy, zc) Es[(c) * L::E_STRIDE + (yy) * EW + (zc)]
 #define EN_AT(c, yy, zc) En[(c) * L::E_STRIDE + (yy) * EW + (zc)]
 #define H_AT(c, yy, zc) Hs[(c) * L::H_STRIDE + (yy) * HW + (zc)]
@@ -970,10 +976,12 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     }
     // Every thread is done with stage `slot` (this H phase and the previous
     // plane's read it; Cb came along above): refill it now.
-    consumed = l + 1;
-    if (issued < nload && issued < consumed + STAGES) {
-      if (tid == 0) issue(issued);
-      ++issued;
+    if (ONE_BARRIER) {
+      consumed = l + 1;
+      if (issued < nload && issued < consumed + STAGES) {
+        if (tid == 0) issue(issued);
+        ++issued;
+      }
     }
 
     if (!warm) {
@@ -1075,6 +1083,14 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
 #undef EN_AT
 #undef H_AT
 #undef HN_AT
+    if (!ONE_BARRIER) {
+      __syncthreads();  // the H plane and stage `slot` are free again
+      consumed = l + 1;
+      if (issued < nload && issued < consumed + STAGES) {
+        if (tid == 0) issue(issued);
+        ++issued;
+      }
+    }
   }
 #undef PSC
 #undef PSH
