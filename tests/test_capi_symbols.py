@@ -74,3 +74,38 @@ def test_sources_have_no_closed_calls(src):
     text = (ROOT / "jaxphys_b200" / "csrc" / src).read_text()
     assert "BatchAsync" not in text
     assert ".multicast::cluster" not in text
+
+
+STRUCTS = {"jxf_grid3d_desc": "Grid3DDesc", "jxf_grid3d_info": "Grid3DInfo",
+           "jxf_noalloc_desc": "NoAllocDesc", "jxf_grid2d_desc": "Grid2DDesc"}
+
+
+def test_ctypes_structs_match_header_layout(tmp_path):
+    """The ctypes mirrors of the header's structs have the C compiler's size
+    and field offsets (a C program built from the header prints them)."""
+    import ctypes as C
+    import shutil
+
+    from jaxphys_b200 import _native
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "jaxphys_fdtd.h"',
+             "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in getattr(_native, pyname)._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(line.split()[:2]): int(line.split()[2]) for line in out if line}
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(_native, pyname)
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
