@@ -13,12 +13,17 @@ documented JAX semantics for the way these files call it (out-of-place
 ``jax_enable_x64``), so the fixtures are the reference's algorithm executed
 op for op in FP64.
 
+The waveguide fixture runs ``src/neurosim/em/waveguides.py`` the same way
+(additionally ``linspace``, ``meshgrid``, ``cos`` and ``nan``).
+
 Usage (needs the reference checkout; not run by the tests)::
 
-    python tests/golden/make_golden.py /path/to/jaxphys
+    python tests/golden/make_golden.py /path/to/jaxphys [--only waveguides]
 
 Writes ``tests/golden/ref3d_<case>.npz`` and ``tests/golden/ref2d_<case>.npz``
-plus ``tests/golden/cases.json`` (the inputs of every case).
+plus ``tests/golden/cases.json`` (the inputs of every case), and
+``tests/golden/waveguides.npz`` (cutoffs, propagation constants, mode
+patterns and dispersion curves of three guides).
 """
 
 from __future__ import annotations
@@ -99,6 +104,10 @@ def _make_jax_modules():
     jnp.roll = lambda x, shift, axis=None: _wrap(np.roll(np.asarray(x), shift, axis=axis))
     jnp.exp = lambda x: _wrap(np.exp(x))
     jnp.sin = lambda x: _wrap(np.sin(x))
+    jnp.cos = lambda x: _wrap(np.cos(x))
+    jnp.nan = np.nan
+    jnp.linspace = lambda *a, **k: _wrap(np.linspace(*a, **k))
+    jnp.meshgrid = lambda *a, **k: tuple(_wrap(m) for m in np.meshgrid(*a, **k))
     jnp.sqrt = lambda x: _wrap(np.sqrt(x))
     jnp.abs = lambda x: _wrap(np.abs(x))
     jnp.max = lambda x, *a, **k: np.max(x, *a, **k)
@@ -160,6 +169,43 @@ def load_reference(ref_root: Path):
     f3 = load("neurosim.em.fdtd3d", src / "em" / "fdtd3d.py")
     f2 = load("neurosim.em.fdtd", src / "em" / "fdtd.py")
     return f3, f2
+
+
+def load_reference_waveguides(ref_root: Path):
+    """The reference's waveguides.py on the same stand-in (after load_reference)."""
+    src = ref_root / "src" / "neurosim"
+    spec = importlib.util.spec_from_file_location("neurosim.em.waveguides",
+                                                  src / "em" / "waveguides.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["neurosim.em.waveguides"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# guides (a, b) in metres and the modes / frequencies evaluated on each
+GUIDES = [(0.02286, 0.01016), (0.02, 0.01), (0.016, 0.008)]
+MODES = [("TE", 1, 0), ("TE", 2, 0), ("TE", 0, 1), ("TE", 1, 1), ("TM", 1, 1), ("TM", 2, 1)]
+
+
+def waveguide_fixture(wg_mod):
+    out = {}
+    freqs = np.linspace(2e9, 40e9, 77)
+    for gi, (a, b) in enumerate(GUIDES):
+        wg = wg_mod.RectangularWaveguide(a=a, b=b)
+        for mt, m, n in MODES:
+            key = f"g{gi}_{mt}{m}{n}"
+            out[key + "_fc"] = np.asarray(wg.cutoff_frequency(m, n))
+            fc = wg.cutoff_frequency(m, n)
+            fs = np.array([1.05 * fc, 1.5 * fc, 3.0 * fc])
+            out[key + "_beta"] = np.array([wg.propagation_constant(float(f), m, n) for f in fs])
+            out[key + "_beta_f"] = fs
+            mode = wg.compute_mode(mt, m, n, n_points=21)
+            out[key + "_pattern"] = np.asarray(mode.field_pattern)
+            out[key + "_x"] = np.asarray(mode.x)
+            out[key + "_y"] = np.asarray(mode.y)
+            out[key + "_disp"] = np.asarray(wg.dispersion_relation(m, n, freqs))
+    out["disp_freqs"] = freqs
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -259,8 +305,17 @@ def run_2d(f2, case):
 
 
 def main(argv):
-    ref_root = Path(argv[1]) if len(argv) > 1 else Path("/root/reference")
+    args = [a for a in argv[1:] if not a.startswith("--")]
+    only = argv[argv.index("--only") + 1] if "--only" in argv else None
+    if only is not None and only in args:
+        args.remove(only)
+    ref_root = Path(args[0]) if args else Path("/root/reference")
     f3, f2 = load_reference(ref_root)
+    wg_mod = load_reference_waveguides(ref_root)
+    np.savez_compressed(HERE / "waveguides.npz", **waveguide_fixture(wg_mod))
+    print("waveguides: saved")
+    if only == "waveguides":
+        return
     for case in CASES_3D:
         out = run_3d(f3, case)
         # keep the first, a middle and the last saved frame to bound fixture size

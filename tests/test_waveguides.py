@@ -222,3 +222,27 @@ def test_oracle_te10_guided_and_evanescent():
     assert all(np.all(o.f[c][wall] == 0) for c in range(3))
     near, far, _, _ = oracle_guide(0.5 * fc, 900)
     assert far.max() / near.max() < 1e-2
+
+
+def test_analysis_matches_reference_golden():
+    """Cutoffs, propagation constants, mode patterns and dispersion curves of
+    three guides against the reference's own waveguides.py executed by
+    tests/golden/make_golden.py (bit for bit: the same FP64 operations)."""
+    from pathlib import Path
+
+    g = np.load(Path(__file__).resolve().parent / "golden" / "waveguides.npz")
+    guides = [(0.02286, 0.01016), (0.02, 0.01), (0.016, 0.008)]
+    modes = [("TE", 1, 0), ("TE", 2, 0), ("TE", 0, 1), ("TE", 1, 1), ("TM", 1, 1), ("TM", 2, 1)]
+    for gi, (a, b) in enumerate(guides):
+        wg = RectangularWaveguide(a=a, b=b)
+        for mt, m, n in modes:
+            key = f"g{gi}_{mt}{m}{n}"
+            assert wg.cutoff_frequency(m, n) == float(g[key + "_fc"])
+            beta = [wg.propagation_constant(float(f), m, n) for f in g[key + "_beta_f"]]
+            np.testing.assert_array_equal(beta, g[key + "_beta"])
+            mode = wg.compute_mode(mt, m, n, n_points=21)
+            np.testing.assert_array_equal(mode.field_pattern, g[key + "_pattern"])
+            np.testing.assert_array_equal(mode.x, g[key + "_x"])
+            np.testing.assert_array_equal(mode.y, g[key + "_y"])
+            np.testing.assert_array_equal(wg.dispersion_relation(m, n, g["disp_freqs"]),
+                                          g[key + "_disp"])
