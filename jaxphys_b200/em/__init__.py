@@ -1,8 +1,10 @@
-"""Electromagnetism: the FDTD Maxwell solvers (2D TM and 3D) and waveguide mode ports."""
+"""Electromagnetism: the FDTD Maxwell solvers (2D TM and 3D), waveguide mode ports and
+moving-charge current sources."""
 
 from .fdtd import FDTD2D, EMGrid, PlaneWave, Wall
 from .fdtd3d import FDTD3D, CPMLSpec, DielectricRegion, EMGrid3D, PointSource3D
 from .waveguides import ModeSource3D, RectangularWaveguide, WaveguideMode
+from .charges import MovingCharge3D, charges_from_trajectory
 
 __all__ = [
     "EMGrid",
@@ -17,4 +19,6 @@ __all__ = [
     "RectangularWaveguide",
     "WaveguideMode",
     "ModeSource3D",
+    "MovingCharge3D",
+    "charges_from_trajectory",
 ]

@@ -64,19 +64,22 @@ class PointSource3D:
         position: Source location as (ix, iy, iz) grid indices.
         amplitude: Peak electric field amplitude (V/m).
         polarization: Which E-field component to drive.
-        waveform: "sine" (reference) or "gauss_sine" (Gaussian-modulated
-            sinusoid, extension).
+        waveform: "sine" (reference), "gauss_sine" (Gaussian-modulated
+            sinusoid, extension) or "table" (explicit per-step values,
+            extension).
         width_steps: Gaussian 1/e half-width in time steps ("gauss_sine").
         delay_steps: Pulse centre in time steps; default four widths.
+        samples: ``sources.SampleTable`` of per-step values ("table").
     """
 
     frequency: float
     position: tuple[int, int, int]
     amplitude: float = 1.0
     polarization: Literal["x", "y", "z"] = "z"
-    waveform: Literal["sine", "gauss_sine"] = "sine"
+    waveform: Literal["sine", "gauss_sine", "table"] = "sine"
     width_steps: float = 30.0
     delay_steps: float | None = None
+    samples: Any = None
 
 
 @dataclass(frozen=True)
@@ -192,9 +195,17 @@ class EMGrid3D:
         """Add a point source to the grid (fdtd3d.py:112-120).
 
         Extension: a ``waveguides.ModeSource3D`` (waveguide mode port) adds
-        its plane of point sources."""
+        its plane of point sources; a ``charges.MovingCharge3D`` adds the
+        current deposit of its trajectory (tabulated with this grid's cell
+        size, default time step and current permittivity)."""
         if hasattr(source, "point_sources"):
             for s in source.point_sources(self.size):
+                self.add_source(s)
+            return
+        if hasattr(source, "deposit_sources"):
+            dt = self._dt if self._dt is not None else self.default_dt()
+            for s in source.deposit_sources(self.size, self._dx, dt, self._t_start,
+                                            self.epsilon_r()):
                 self.add_source(s)
             return
         ix, iy, iz = source.position

@@ -9,6 +9,9 @@ update of step ``n``; this module builds the ``wave`` rows.
 * ``"gauss_sine"`` -- extension: Gaussian-modulated sinusoid
   ``exp(-((t_c-t0)/tau)^2) * sin(2*pi*f*(t_c-t0))`` with ``tau = width_steps*dt``
   and ``t0 = delay_steps*dt`` (default delay: four widths).
+* ``"table"`` -- extension: explicit per-step values (a ``SampleTable``;
+  sample n is the value of step n, zero past the end), e.g. the current
+  deposit of a moving charge (``charges.py``).
 """
 
 from __future__ import annotations
@@ -16,8 +19,23 @@ from __future__ import annotations
 import numpy as np
 
 
+class SampleTable:
+    """Per-step source values (float64), compared by identity so that a
+    table is one waveform row however many sources share it."""
+
+    __slots__ = ("values",)
+
+    def __init__(self, values):
+        self.values = np.ascontiguousarray(values, dtype=np.float64)
+
+
 def waveform_key(src) -> tuple:
     kind = getattr(src, "waveform", "sine")
+    if kind == "table":
+        table = getattr(src, "samples", None)
+        if not isinstance(table, SampleTable):
+            raise ValueError("a 'table' waveform needs samples=SampleTable(values)")
+        return ("table", table)
     if kind == "sine":
         return ("sine", float(src.frequency))
     if kind == "gauss_sine":
@@ -30,6 +48,11 @@ def waveform_key(src) -> tuple:
 
 def tabulate(key: tuple, n_samples: int, dt: float, t_start: float) -> np.ndarray:
     """Samples of one waveform at absolute steps 0..n_samples-1 (FP64)."""
+    if key[0] == "table":
+        out = np.zeros(n_samples, dtype=np.float64)
+        v = key[1].values[:n_samples]
+        out[:len(v)] = v
+        return out
     n = np.arange(n_samples, dtype=np.float64)
     t_c = t_start + n * dt
     if key[0] == "sine":

@@ -92,6 +92,15 @@ def waveform_values(src: dict, n_steps: int, dt: float, t_start: float,
         t0 = float(src["delay_steps"]) * dt
         u = t_c - t0
         return amp * (np.exp(-((u / tau) ** 2)) * np.sin(2.0 * np.pi * f0 * u))
+    if kind == "table":
+        # extension: explicit per-step values (sample n is added at step n;
+        # zero past the end of the table)
+        samples = np.asarray(src["samples"], dtype=np.float64)
+        out = np.zeros(n_steps, dtype=np.float64)
+        lo, hi = step0, min(step0 + n_steps, len(samples))
+        if hi > lo:
+            out[:hi - lo] = samples[lo:hi]
+        return amp * out
     raise ValueError(f"unknown waveform kind {kind!r}")
 
 
