@@ -14,6 +14,8 @@ the hand-written CUDA adjoint of the FDTD step (sqrt(T) checkpointing):
     >>> res = optimize(objective, theta0, learning_rate=0.05, max_iterations=20,
     ...                method="adam")
 
+``sensitivity`` is the reference's Jacobian helper (``optimize.py:210-228``).
+
 Same arguments, defaults, update rules and stopping test as the reference:
 gradient descent x <- x - lr g; Adam with beta1 = 0.9, beta2 = 0.999,
 eps = 1e-8 and bias correction (``optimize.py:142-207``); convergence when
@@ -86,9 +88,13 @@ def optimize(
     """
     if method not in ("gradient_descent", "adam"):
         raise ValueError(f"unknown method {method!r}")
-    x = torch.as_tensor(initial_guess).detach().clone()
-    if not torch.is_floating_point(x):
-        x = x.to(torch.float64)
+    # Python numbers, lists and arrays become float64 as in the reference
+    # (optimize.py:83, jnp.asarray(..., float64)); a floating tensor keeps its
+    # dtype and device (e.g. float32 parameters of a CUDA objective)
+    if isinstance(initial_guess, torch.Tensor) and torch.is_floating_point(initial_guess):
+        x = initial_guess.detach().clone()
+    else:
+        x = torch.as_tensor(initial_guess, dtype=torch.float64).detach().clone()
     logger.info("Starting optimization: method=%s, lr=%.2e, max_iter=%d", method,
                 learning_rate, max_iterations)
     traj = [x.clone()] if track_trajectory else []
@@ -125,3 +131,15 @@ def optimize(
             traj.append(x.clone())
     logger.warning("Optimization did not converge after %d iterations", max_iterations)
     return result(max_iterations, False)
+
+
+def sensitivity(simulation_fn: Any, params) -> torch.Tensor:
+    """Jacobian d(outputs)/d(params) of a simulation (``optimize.py:210-228``).
+
+    ``params`` becomes a float64 tensor (as the reference's ``jnp.asarray(...,
+    dtype=float64)``); the Jacobian comes from torch autograd, so a
+    ``simulation_fn`` built on ``probe_traces`` differentiates through the
+    CUDA adjoint.  Shape: outputs' shape + params' shape.
+    """
+    p = torch.as_tensor(params, dtype=torch.float64).detach()
+    return torch.autograd.functional.jacobian(simulation_fn, p)

@@ -92,3 +92,46 @@ def test_inverse_design_through_adjoint(cuda):
     assert res.fun < f0, (res.fun, f0)
     assert res.trajectory.shape == (5, 6, 6, 4)
     assert torch.isfinite(res.x).all()
+
+
+# The reference's own optimizer tests (tests/test_optimize.py:14-80 and
+# tests/test_edge_cases.py:1398-1440), on torch tensors.
+
+
+def test_reference_quadratic_minimum():
+    res = optimize(lambda x: (x - 3.0) ** 2, 0.0, learning_rate=0.1, max_iterations=1000)
+    assert res.converged
+    assert float(res.x) == pytest.approx(3.0, abs=1e-4)
+    assert res.fun < 1e-6
+
+
+def test_reference_adam():
+    res = optimize(lambda x: (x - 5.0) ** 2 + 1.0, 0.0, learning_rate=0.1, max_iterations=1000,
+                   method="adam")
+    assert float(res.x) == pytest.approx(5.0, abs=0.1)
+
+
+def test_reference_trajectory_and_multivariate():
+    res = optimize(lambda x: x ** 2, 10.0, learning_rate=0.1, max_iterations=100,
+                   track_trajectory=True)
+    assert res.trajectory is not None and res.trajectory.shape[0] > 1
+    target = torch.tensor([1.0, 2.0], dtype=torch.float64)
+    res = optimize(lambda x: torch.sum((x - target) ** 2), torch.zeros(2, dtype=torch.float64),
+                   learning_rate=0.1, max_iterations=1000)
+    assert torch.allclose(res.x, target, atol=0.1)
+
+
+def test_reference_edge_cases():
+    res = optimize(lambda x: x ** 2, 0.0, learning_rate=0.1, tolerance=1e-8)
+    assert res.converged and res.n_iterations == 0
+    res = optimize(lambda x: (x - 100.0) ** 2, 0.0, learning_rate=0.001, max_iterations=5)
+    assert not res.converged and res.n_iterations == 5
+
+
+def test_reference_sensitivity():
+    from jaxphys_b200.optimize import sensitivity
+
+    s = sensitivity(lambda p: p ** 2, [3.0])
+    assert s.shape == (1, 1) and float(s[0, 0]) == pytest.approx(6.0, abs=1e-6)
+    j = sensitivity(lambda p: torch.stack([p[0] * p[1], p[1] ** 3]), [2.0, 3.0])
+    np.testing.assert_allclose(j.numpy(), [[3.0, 2.0], [0.0, 27.0]])
