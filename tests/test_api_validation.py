@@ -108,6 +108,11 @@ def test_emconfig():
         EMConfig(boundary="invalid")
     with pytest.raises(ValidationError):
         EMGrid(size=(20, 20), boundary="bogus")
+    # tests/test_edge_cases.py:738-752 of the reference
+    with pytest.raises(ValidationError):
+        EMConfig(resolution=0.0)
+    with pytest.raises(ValidationError):
+        EMConfig(courant_number=1.5)
 
 
 def test_exception_hierarchy():
