@@ -54,10 +54,6 @@ WORKLOADS = {
 }
 BAND_WEIGHTS = ROOT / "jaxphys_b200" / "em" / "band_weights.npz"
 
-# DRAM bytes per leapfrog step (CPML shell launch + interior launch) from the
-# ncu capture of the same workload and launch shape
-# (profiles/k3d_tma_cpml_128cubed_bench_c2.md); None where not captured.
-NCU_TRAFFIC = {"c2": 81.7e6, "c1": None, "c3": None}
 
 
 def make_inputs(name: str, seed: int = 0):
@@ -498,10 +494,16 @@ def cpu_baseline(workload: str, budget_s: float = 10.0, steps: int | None = None
     return {"value": round(v, 4), "unit": "Gcell/s", "cores": num_threads(), "kind": "port",
             "sample": f"{wname}: {steps} leapfrog steps of the same grid, source and "
                       f"permittivity (FP64, oracle/cpu_fdtd.c, {num_threads()} threads)",
-            "seconds": round(el, 2)}
+            "seconds": round(el, 4)}
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the CPU restatement of the reference step (FP64 C,
+    every host thread) on the same workload.  A bench step is the whole
+    workload (all its leapfrog steps) when that takes at most
+    ``JXF_REF_STEP_SECONDS`` (default 12 s) on this host, else the longest
+    prefix that fits; ``value`` is the cell updates of all timed steps over
+    their total time."""
     if rank != 0:
         return
     if args.workload == "c5":
@@ -510,17 +512,19 @@ def run_reference(args, world, rank):
                           "the c1/c2/c3 workloads"}), flush=True)
         return
     n, nsteps, pml, wname = WORKLOADS[args.workload]
-    # each bench step: a bounded sample of the workload on the host cores
-    sample = max(4, min(nsteps, int(os.environ.get("JXF_REF_SAMPLE_STEPS", "20"))))
+    budget = float(os.environ.get("JXF_REF_STEP_SECONDS", "12"))
+    probe = cpu_baseline(args.workload, steps=4)
+    per_step = probe["seconds"] / 4
+    sample = max(4, min(nsteps, int(budget / max(per_step, 1e-9))))
     for _ in range(args.warmup):
         cpu_baseline(args.workload, steps=2)
-    times = []
+    times, updates = [], 0
     res = None
     for _ in range(args.steps):
-        t0 = time.perf_counter()
         res = cpu_baseline(args.workload, steps=sample)
-        times.append(time.perf_counter() - t0)
-    value = statistics.mean([r for r in [res["value"]]])
+        times.append(res["seconds"])
+        updates += n ** 3 * sample
+    value = round(updates / sum(times) / 1e9, 4)
     line = {
         "metric": "FDTD3D Gcell-updates/s",
         "value": value,
@@ -533,9 +537,10 @@ def run_reference(args, world, rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded eps_r sphere, pulsed dipole, seeded probes)",
+        "data": "synthetic (seeded eps_r map, pulsed dipole, seeded probes)",
         "config": {"workload": wname, "cells": n ** 3, "leapfrog_steps_per_step": sample,
-                   "boundary": "cpml", "pml_layers": pml},
+                   "boundary": "cpml", "pml_layers": pml,
+                   "same_config": sample == nsteps},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "Gcell/s", "cores": res["cores"], "kind": "port",
                          "sample": res["sample"]},

@@ -275,7 +275,8 @@ int jxf_grid3d_check_finite(jxf_grid3d* g, void* stream);
  * the library until exit) instead of allocations.  Limit: at most
  * JXF_NOALLOC_MAX_CELLS cells, at most 4096 per axis, nz % 4 == 0; larger
  * grids are rejected with JXF_ERR_INVALID.  cb: device per-cell
- * dt/(eps0 dx eps_r) (float32) or NULL for vacuum.  The first call on a
+ * dt/(eps0 dx eps_r) (float32) or NULL for vacuum.  Every pointer must be
+ * 16-byte aligned (JXF_ERR_INVALID otherwise).  The first call on a
  * device resolves the scratch address (cudaGetSymbolAddress), so make it
  * before any stream capture.  All calls share the scratch: calls that
  * overlap on the GPU (other streams, other threads) race.  Synchronises

@@ -2885,6 +2885,12 @@ extern "C" int jxf_grid3d_run_noalloc(const jxf_noalloc_desc* desc, float* const
   const jxf_noalloc_desc d = *desc;
   for (int k = 0; k < 6; ++k)
     if (!fields[k]) return fail(JXF_ERR_INVALID, "field pointer %d is null", k);
+  // the TMA tensor maps need 16-byte aligned base addresses
+  for (int k = 0; k < 6; ++k)
+    if (reinterpret_cast<uintptr_t>(fields[k]) % 16 != 0)
+      return fail(JXF_ERR_INVALID, "field pointer %d is not 16-byte aligned", k);
+  if (cb && reinterpret_cast<uintptr_t>(cb) % 16 != 0)
+    return fail(JXF_ERR_INVALID, "cb pointer is not 16-byte aligned");
   if (n_steps < 0) return fail(JXF_ERR_INVALID, "n_steps must be >= 0");
   if (d.nx < 2 || d.ny < 2 || d.nz < 2)
     return fail(JXF_ERR_INVALID, "grid must be at least 2 cells per axis");

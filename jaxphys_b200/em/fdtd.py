@@ -22,7 +22,7 @@ import numpy as np
 from .. import _native as nat
 from ..config import EMConfig
 from ..exceptions import ConfigurationError
-from ..state import EMFieldHistory
+from ..state import EMFieldHistory, resolve_output, to_jax
 from . import sources as wf
 
 logger = logging.getLogger(__name__)
@@ -195,11 +195,16 @@ class EMGrid:
         t_span: tuple[float, float] = (0.0, 1e-8),
         dt: float | None = None,
         save_every: int = 10,
-        output: Literal["torch", "numpy"] = "torch",
+        output: Literal["torch", "numpy", "jax", "auto"] = "torch",
     ) -> EMFieldHistory:
-        """Run the FDTD simulation (fdtd.py:193-386)."""
+        """Run the FDTD simulation (fdtd.py:193-386).
+
+        output: "torch" (tensors), "numpy", "jax" (JAX arrays through DLPack,
+        the reference's result type) or "auto" (JAX when importable, else
+        torch)."""
         import torch
 
+        output = resolve_output(output)
         dx = self._dx
         nx, ny = self._nx, self._ny
         dt = self.default_dt() if dt is None else float(dt)
@@ -233,6 +238,11 @@ class EMGrid:
         if output == "numpy":
             return EMFieldHistory(t, hist[0].cpu().numpy(), hist[1].cpu().numpy(),
                                   hist[2].cpu().numpy(), gx, gy)
+        if output == "jax":
+            import jax.numpy as jnp
+
+            return EMFieldHistory(jnp.asarray(t), *[to_jax(h) for h in hist], jnp.asarray(gx),
+                                  jnp.asarray(gy))
         return EMFieldHistory(torch.from_numpy(t), hist[0], hist[1], hist[2],
                               torch.from_numpy(gx), torch.from_numpy(gy))
 

@@ -32,7 +32,7 @@ import numpy as np
 
 from .. import _native as nat
 from ..exceptions import ConfigurationError, SimulationError
-from ..state import EMFieldHistory3D
+from ..state import EMFieldHistory3D, resolve_output, to_jax
 from . import sources as wf
 
 logger = logging.getLogger(__name__)
@@ -537,7 +537,7 @@ class EMGrid3D:
         t_span: tuple[float, float] = (0.0, 5e-9),
         dt: float | None = None,
         save_every: int = 20,
-        output: Literal["torch", "numpy"] = "torch",
+        output: Literal["torch", "numpy", "jax", "auto"] = "torch",
         history: Literal["device", "host"] = "device",
     ) -> EMFieldHistory3D:
         """Run the 3D FDTD simulation (fdtd3d.py:169-417).
@@ -552,9 +552,14 @@ class EMGrid3D:
         slots and from there to the host on a side stream while the next
         steps run, so device memory holds two frames whatever the number of
         frames (the reference materialises every step, fdtd3d.py:371-404).
+
+        output: "torch" (tensors), "numpy", "jax" (JAX arrays through DLPack,
+        the reference's result type) or "auto" (JAX when importable, else
+        torch).
         """
         import torch
 
+        output = resolve_output(output)
         dx = self._dx
         nx, ny, nz = self.size
         if dt is None:
@@ -624,6 +629,11 @@ class EMGrid3D:
         if output == "numpy":
             arrs = [h.cpu().numpy() for h in hist]
             return EMFieldHistory3D(t, *arrs, gx, gy, gz)
+        if output == "jax":
+            import jax.numpy as jnp
+
+            return EMFieldHistory3D(jnp.asarray(t), *[to_jax(h) for h in hist], jnp.asarray(gx),
+                                    jnp.asarray(gy), jnp.asarray(gz))
         return EMFieldHistory3D(torch.from_numpy(t), *hist, torch.from_numpy(gx),
                                 torch.from_numpy(gy), torch.from_numpy(gz))
 

@@ -521,60 +521,3 @@ def train_band(seed: int = 0, n_cases: int = 8, size_range=(18, 40), n_steps: in
                 f"largest field-norm ratio to the reference {worst:.3g}")
         fit(dagger_schedule, f"round {r}")
     return model
-
-
-def _main(argv=None) -> None:
-    """Run a batch of boxes with the shipped band and report its throughput
-    (also the target of the band kernel's profiles)."""
-    import argparse
-    import time
-
-    import torch
-
-    from .batch import FDTDBatch
-
-    ap = argparse.ArgumentParser(prog="python -m jaxphys_b200.em.learned",
-                                 description="batch of grids with the shipped learned band")
-    ap.add_argument("--grids", type=int, default=6)
-    ap.add_argument("--size", type=int, default=120, help="interior side")
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--seed", type=int, default=5)
-    ap.add_argument("--train", type=int, default=0, metavar="ITERS",
-                    help="instead: collect CPML traces of one box and run ITERS Adam steps")
-    a = ap.parse_args(argv)
-    rng = np.random.default_rng(a.seed)
-    if a.train > 0:
-        m = LearnedBand(seed=a.seed)
-        collect_traces(m, random_case(rng, (32, 30, 34), eps_range=(1.0, 6.0)), n_steps=200,
-                       noise=0.03, seed=a.seed)
-        rows = int(m.dataset_size().sum())
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        loss = m.train(a.train, batch_rows=8192, lr=1e-3, seed=a.seed)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        print(f"{rows} rows; {a.train} Adam steps of 6 x 8192 rows in {dt:.3f} s "
-              f"({a.train * 6 * 8192 / dt / 1e6:.1f} M rows/s); loss {loss[0]:.4g} -> {loss[-1]:.4g}")
-        m.close()
-        return
-    cases = [random_case(rng, (a.size,) * 3, eps_range=(1.0, 6.0)) for _ in range(a.grids)]
-    grids = []
-    for c in cases:
-        g = c.grid(BAND_LAYERS, "pec", 0)
-        g.prepare()
-        grids.append(g)
-    b = FDTDBatch(grids)
-    b.set_band(default_band())
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    b.run(a.steps, use_graph=False)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    cells = sum(int(np.prod(g.size)) for g in grids)
-    default_band().check()
-    print(f"{a.grids} grids, {cells} cells, {a.steps} steps: {cells * a.steps / dt / 1e9:.2f} "
-          f"Gcell-updates/s (wall clock, first run)")
-
-
-if __name__ == "__main__":
-    _main()

@@ -53,3 +53,43 @@ class EMFieldHistory3D:
     grid_x: Any
     grid_y: Any
     grid_z: Any
+
+
+def jax_available() -> bool:
+    """True when ``jax`` can be imported in this process."""
+    try:
+        import jax  # noqa: F401
+    except Exception:
+        return False
+    return True
+
+
+def to_jax(t):
+    """A torch tensor as a JAX array.
+
+    Through DLPack (no copy) when the JAX backend can address the tensor's
+    device; otherwise through host memory (a CPU-only jaxlib cannot import a
+    CUDA buffer).  The reference returns JAX arrays from ``simulate``
+    (``src/neurosim/state.py:388-414``).
+    """
+    import jax
+    import jax.numpy as jnp
+
+    try:
+        return jax.dlpack.from_dlpack(t.contiguous())
+    except Exception:
+        return jnp.asarray(t.detach().cpu().numpy())
+
+
+def resolve_output(output: str) -> str:
+    """``"auto"``: JAX arrays when JAX is importable (the reference's result
+    type), torch tensors otherwise."""
+    from .exceptions import ConfigurationError
+
+    if output == "auto":
+        return "jax" if jax_available() else "torch"
+    if output not in ("torch", "numpy", "jax"):
+        raise ConfigurationError(f"output must be 'auto', 'torch', 'numpy' or 'jax', got {output!r}")
+    if output == "jax" and not jax_available():
+        raise ConfigurationError("output='jax' needs the jax package")
+    return output

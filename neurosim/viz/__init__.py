@@ -1,0 +1,3 @@
+"""Field viewers under the reference's module path (``src/neurosim/viz/fields.py``)."""
+
+from .fields import animate_field, plot_field_snapshot  # noqa: F401

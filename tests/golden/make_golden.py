@@ -309,7 +309,10 @@ def main(argv):
     only = argv[argv.index("--only") + 1] if "--only" in argv else None
     if only is not None and only in args:
         args.remove(only)
-    ref_root = Path(args[0]) if args else Path("/root/reference")
+    if not args:
+        raise SystemExit("usage: python tests/golden/make_golden.py <reference checkout> "
+                         "[--only waveguides]")
+    ref_root = Path(args[0])
     f3, f2 = load_reference(ref_root)
     wg_mod = load_reference_waveguides(ref_root)
     np.savez_compressed(HERE / "waveguides.npz", **waveguide_fixture(wg_mod))

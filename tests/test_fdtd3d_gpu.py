@@ -299,6 +299,59 @@ def test_config2_sphere_checksum(cuda):
     assert rel_l2(np.vstack([tr1, tr2]), np.vstack([p1, p2])) <= TOL
 
 
+def _rel_l2_by_component(got_fn, ref6, comps):
+    """Relative L2 of a vector field over the components ``comps``, summed
+    one component at a time (a 512^3 FP64 stack would take 3 GB of host
+    memory per family)."""
+    num = den = 0.0
+    for c in comps:
+        g = np.asarray(got_fn(c), np.float64)
+        num += float(np.sum((g - ref6[c]) ** 2))
+        den += float(np.sum(ref6[c] ** 2))
+        del g
+    return float(np.sqrt(num / den))
+
+
+def test_config3_512_cpml12_smooth_eps(cuda):
+    """Config 3: 512^3 FP32, 200 steps, 12-cell CPML (m=3, R0=1e-6), eps_r
+    from seeded uniform noise smoothed by a Gaussian (sigma = 6 cells) and
+    rescaled to [1, 12], Gaussian-modulated Ez dipole at the centre (f0 =
+    0.05/dt, width 30 steps), 16 seeded interior Ez probes.  Checked against
+    the FP64 C oracle: probe traces over the whole run and the E and H fields
+    after step 200 (the pulse is still inside the box), relative L2 <= 1e-5
+    (tolerance of the 3D FP32 path)."""
+    from scipy.ndimage import gaussian_filter
+
+    from oracle.cpu_oracle import Oracle3DC
+
+    n, steps, pml = 512, 200, 12
+    dt = rn.default_dt_3d(1.0)
+    rng = np.random.default_rng(3)
+    u = gaussian_filter(rng.random((n, n, n), dtype=np.float32), sigma=6, mode="wrap")
+    u = (u - u.min()) / (u.max() - u.min())
+    eps = (1.0 + 11.0 * u.astype(np.float64))
+    del u
+    probes = _cfg_probes(n, 16, seed=3)
+    src = [_gauss((n // 2, n // 2, n // 2), width=30.0)]
+    g = _cpml_grid("auto", (n, n, n), None, src, probes, n_pml=pml)
+    g.set_permittivity(eps)
+    g.prepare(dt=dt)
+    assert g.info()["path"] == 2, "512^3 CPML must run on the TMA path"
+    tr = to_np(g.run(steps))
+    g.check()
+    spec = rn.Spec3D(size=(n, n, n), dx=1.0, boundary="cpml", pml_layers=pml, eps_r=eps,
+                     sources=[dict(position=(n // 2,) * 3, polarization="z", amplitude=1.0,
+                                   kind="gauss_sine", frequency=0.05 / dt, width_steps=30.0,
+                                   delay_steps=120.0)], probes=probes)
+    del eps
+    o = Oracle3DC(spec, dt=dt)
+    out = o.run(steps)
+    assert rel_l2(tr, out["probes"]) <= TOL
+    eE = _rel_l2_by_component(lambda c: to_np(g.field(COMPS[c])), o.f, (0, 1, 2))
+    eH = _rel_l2_by_component(lambda c: to_np(g.field(COMPS[c])), o.f, (3, 4, 5))
+    assert eE <= TOL and eH <= TOL, (eE, eH)
+
+
 def test_finite_check_raises(cuda):
     from jaxphys_b200 import EMGrid3D, NumericalInstabilityError, PointSource3D
 
