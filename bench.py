@@ -56,6 +56,18 @@ BAND_WEIGHTS = ROOT / "jaxphys_b200" / "em" / "band_weights.npz"
 
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, ncu) per leapfrog
+# step of a workload, keyed by the launch shape they were captured at: a
+# figure applies only when the run's autotuned launch is that shape.
+NCU_TRAFFIC: dict = {}
+
+
+def ncu_traffic(workload: str, launch: dict):
+    key = (workload, launch["tma_config"], launch["x_chunk"], launch["axis_split"],
+           launch["blocked_config"], launch["blocked_x_chunk"])
+    return NCU_TRAFFIC.get(key)
+
+
 def make_inputs(name: str, seed: int = 0):
     """Permittivity map, source and probes of a workload (seeded)."""
     n, steps, pml, _ = WORKLOADS[name]
@@ -174,15 +186,21 @@ def dist_setup():
     return world, rank, local, pg
 
 
-def run_ours(args, world, rank, local, pg):
+def run_ours(args, world, rank, local, pg, workload=None, steps=None, warmup=None,
+             with_cpu=True, emit=True):
+    """One independent grid of a single-grid workload per rank; returns the
+    JSON line (printed by rank 0 when ``emit``)."""
     import torch
 
     from jaxphys_b200 import CPMLSpec, EMGrid3D, PointSource3D
 
+    workload = workload or args.workload
+    n_timed = args.steps if steps is None else steps
+    n_warm = args.warmup if warmup is None else warmup
     torch.cuda.set_device(local)
     dev = torch.device(f"cuda:{local}")
-    n, nsteps, pml, wname = WORKLOADS[args.workload]
-    eps, probes = make_inputs(args.workload, seed=rank)
+    n, nsteps, pml, wname = WORKLOADS[workload]
+    eps, probes = make_inputs(workload, seed=rank)
     g = EMGrid3D(size=(n, n, n), resolution=1.0, boundary="cpml", pml_layers=pml,
                  cpml=CPMLSpec(order=3.0, r0=1e-6), device=local)
     dt = g.default_dt()
@@ -205,7 +223,7 @@ def run_ours(args, world, rank, local, pg):
         if pg is not None:
             pg.barrier()
 
-    for _ in range(args.warmup):
+    for _ in range(n_warm):
         one_step()
     g.check()
     barrier()
@@ -214,11 +232,11 @@ def run_ours(args, world, rank, local, pg):
     sampler = ClockSampler(local)
     sampler.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
+          for _ in range(n_timed)]
     kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
+           for _ in range(n_timed)]
     barrier()
-    for k in range(args.steps):
+    for k in range(n_timed):
         flush.fill_(k & 0xFF)
         ev[k][0].record(stream)
         g.reset()
@@ -256,8 +274,8 @@ def run_ours(args, world, rank, local, pg):
     e2e_step()
     barrier()
     e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            for _ in range(args.steps)]
-    for k in range(args.steps):
+            for _ in range(n_timed)]
+    for k in range(n_timed):
         flush.fill_(k & 0xFF)
         e_ev[k][0].record(stream)
         e2e_step()
@@ -272,7 +290,7 @@ def run_ours(args, world, rank, local, pg):
     d2h = probe_host.numel() * 4
 
     cells = n ** 3
-    updates = cells * nsteps * args.steps * world
+    updates = cells * nsteps * n_timed * world
     value = updates / (total_ms * 1e-3) / 1e9
     e2e_value = updates / (e2e_ms * 1e-3) / 1e9
 
@@ -285,16 +303,26 @@ def run_ours(args, world, rank, local, pg):
     bytes_per_launch = cells * b_cell
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = NCU_TRAFFIC.get(args.workload)
+    launch = {"tma_config": info["tma_config"], "x_chunk": info["x_chunk"],
+              "axis_split": info["axis_split"], "blocked_config": info["blocked_config"],
+              "blocked_x_chunk": info["blocked_x_chunk"]}
+    traffic = ncu_traffic(workload, launch)
+    blocked = info["blocked_config"] >= 0
+    if blocked:
+        # pairs of steps per blocked pass (+ one ordinary step for an odd count)
+        launches = (nsteps // 2) * info["blocked_kernels_per_pass"] + \
+            (nsteps % 2) * g.kernels_per_step() + 1
+    else:
+        launches = nsteps * g.kernels_per_step() + 1
 
     line = {
         "metric": "FDTD3D Gcell-updates/s",
         "value": round(value, 3),
         "unit": "Gcell/s",
         "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(total_ms / args.steps, 4),
+        "steps": n_timed,
+        "warmup": n_warm,
+        "ms_per_step": round(total_ms / n_timed, 4),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -305,23 +333,27 @@ def run_ours(args, world, rank, local, pg):
                    "path": "tma" if info["path"] == 2 else "generic",
                    "tile": [info["tile_z"], info["tile_y"], info["rows_per_thread"],
                             info["stages"], info["x_chunk"]],
-                   "launch": {"tma_config": info["tma_config"], "x_chunk": info["x_chunk"],
-                              "axis_split": info["axis_split"]},
+                   "launch": launch,
                    "parallelism": f"independent grid per GPU x{world}"},
         "e2e": {"value": round(e2e_value, 3), "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": peak_kind, "bytes_per_cell_update": round(b_cell, 2),
-                     "kernel": "k3d_tma step (every launch of one leapfrog step)",
+                     "kernel": ("k3d_tb2 two-level blocked pass (every launch of a pass), "
+                                "per leapfrog step" if blocked else
+                                "k3d_tma step (every launch of one leapfrog step)"),
                      "ms_per_leapfrog_step": round(per_launch_ms, 5)},
-        "gpu_launches": (nsteps * g.kernels_per_step() + 1) * args.steps,
+        "gpu_launches": launches * n_timed,
         "clocks": clocks,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.workload, budget_s=args.cpu_seconds)
-    if rank == 0:
+    if rank == 0 and world == 1 and with_cpu and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(workload, budget_s=args.cpu_seconds)
+    g._release()
+    del flush
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
 def c5_cases(seed: int = 5, n_grids: int = 64):
@@ -343,11 +375,16 @@ def c5_cases(seed: int = 5, n_grids: int = 64):
     return cases
 
 
-def run_batch(args, world, rank, local, pg):
+def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=None,
+              emit=True):
     """c5: the same 64-grid batch with the learned 3-cell band, with 10-cell
     CPML, with the CPML of equal measured error (4 cells) and with bare PEC
     walls.  value = interior cell updates per second of the learned run."""
     import torch
+
+    n_timed = args.steps if steps is None else steps
+    n_warm = args.warmup if warmup is None else warmup
+    n_refl = args.reflection if reflection is None else reflection
 
     from jaxphys_b200.em.batch import FDTDBatch
     from jaxphys_b200.em.learned import BAND_LAYERS, LearnedBand, reflection_db, train_band
@@ -385,7 +422,7 @@ def run_batch(args, world, rank, local, pg):
     for kind in ("learned", "cpml10", "cpml4", "pec"):
         grids, b = build(kind)
         cells = sum(int(np.prod(g.size)) for g in grids)
-        for _ in range(max(args.warmup, 1)):
+        for _ in range(max(n_warm, 1)):
             b.reset()
             b.run(nsteps)
         barrier()
@@ -393,8 +430,8 @@ def run_batch(args, world, rank, local, pg):
             sampler = ClockSampler(local)
             sampler.start()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-        for k in range(args.steps):
+              for _ in range(n_timed)]
+        for k in range(n_timed):
             b.reset()
             ev[k][0].record(stream)
             b.run(nsteps)
@@ -408,20 +445,20 @@ def run_batch(args, world, rank, local, pg):
             ms = float(t.item())
         for g in grids[:2]:
             g.check()
-        results[kind] = {"ms_per_step": round(ms / args.steps, 3), "grid_cells": cells,
-                         "interior_gcell_s": round(interior * nsteps * args.steps * world / ms / 1e6, 3),
-                         "grid_gcell_s": round(cells * nsteps * args.steps * world / ms / 1e6, 3)}
+        results[kind] = {"ms_per_step": round(ms / n_timed, 3), "grid_cells": cells,
+                         "interior_gcell_s": round(interior * nsteps * n_timed * world / ms / 1e6, 3),
+                         "grid_gcell_s": round(cells * nsteps * n_timed * world / ms / 1e6, 3)}
         if kind == "learned":
             results[kind]["clocks"] = clocks
             # per leapfrog step: batched H, E, sources, band inference, band apply
-            launches = 5 * nsteps * args.steps
+            launches = 5 * nsteps * n_timed
         b.close()
         for g in grids:
             g._release()
     model.check()
     refl = {}
-    if rank == 0 and args.reflection > 0:
-        small = sorted(range(len(cases)), key=lambda i: np.prod(cases[i].size))[:args.reflection]
+    if rank == 0 and n_refl > 0:
+        small = sorted(range(len(cases)), key=lambda i: np.prod(cases[i].size))[:n_refl]
         for i in small:
             r = reflection_db(cases[i], nsteps, model=model, cpml_layers=(4, 10), every=10)
             refl[str(cases[i].size)] = {k: round(v, 2) for k, v in r.items()}
@@ -440,8 +477,8 @@ def run_batch(args, world, rank, local, pg):
         "value": lr["interior_gcell_s"],
         "unit": "Gcell/s",
         "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
+        "steps": n_timed,
+        "warmup": n_warm,
         "ms_per_step": lr["ms_per_step"],
         "higher_is_better": True,
         "scaling": "weak",
@@ -462,8 +499,9 @@ def run_batch(args, world, rank, local, pg):
         "gpu_launches": launches,
         "clocks": lr.pop("clocks"),
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
 def cpu_baseline(workload: str, budget_s: float = 10.0, steps: int | None = None):
@@ -550,6 +588,25 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def secondary(args, world, rank, local, pg):
+    """Config 3 (512^3, 12-cell CPML, eps_r in [1, 12]) and config 5 (64
+    batched grids, learned band against CPML) measured in the same run as the
+    headline line, with their own short step counts (3 and 2 timed steps)."""
+    out = {}
+    c3 = run_ours(args, world, rank, local, pg, workload="c3", steps=3, warmup=1,
+                  with_cpu=False, emit=False)
+    out["c3"] = {k: c3[k] for k in ("value", "unit", "ms_per_step", "steps", "warmup",
+                                    "roofline", "gpu_launches", "clocks", "e2e")}
+    out["c3"]["config"] = c3["config"]
+    c5 = run_batch(args, world, rank, local, pg, steps=2, warmup=1, reflection=2, emit=False)
+    out["c5"] = {k: c5[k] for k in ("metric", "value", "unit", "ms_per_step", "steps", "warmup",
+                                    "compare", "speedup_vs_cpml10",
+                                    "speedup_vs_cpml4_equal_error", "reflection_db",
+                                    "roofline", "gpu_launches", "clocks", "dtype")}
+    out["c5"]["config"] = c5["config"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -561,6 +618,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reflection", type=int, default=2,
                     help="c5: grids whose reflection is measured against a padded reference")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="default workload: skip the config-3 and config-5 measurements")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     try:
@@ -568,6 +627,10 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "c5":
             run_batch(args, world, rank, local, pg)
+        elif args.workload == "c2" and world == 1 and not args.no_secondary:
+            line = run_ours(args, world, rank, local, pg, emit=False)
+            line["secondary"] = secondary(args, world, rank, local, pg)
+            print(json.dumps(line), flush=True)
         else:
             run_ours(args, world, rank, local, pg)
     finally:

@@ -86,6 +86,9 @@ typedef struct {
   int32_t shell_blocks, interior_blocks;  /* CPML region split (TMA path) */
   int32_t tma_config;         /* launch-shape registry entry (TMA path)   */
   int32_t axis_split;         /* single-axis CPML shell split on (1)/off  */
+  int32_t blocked_config;     /* two-level blocked registry entry, or -1  */
+  int32_t blocked_x_chunk;    /* planes per block of the blocked launch   */
+  int32_t blocked_kernels_per_pass; /* launches per blocked pass (2 steps) */
 } jxf_grid3d_info;
 
 int jxf_grid3d_create(const jxf_grid3d_desc* desc, jxf_grid3d** out);
@@ -102,6 +105,14 @@ int jxf_grid3d_set_launch(jxf_grid3d* g, int32_t cfg, int32_t x_chunk);
  * arrays instead of 12, smaller shared memory); the autotuner chooses it per
  * grid shape, this pins it (with jxf_grid3d_set_launch). */
 int jxf_grid3d_set_axis_split(jxf_grid3d* g, int32_t on);
+/* Two-level temporal blocking (TMA path; replaces two iterations of the
+ * reference's scan body, fdtd3d.py:280-379, per pass over the fields): cfg in
+ * [0, jxf_num_blocked_configs()) advances pairs of steps with one blocked
+ * pass each (an odd remainder takes one ordinary step), x_chunk planes per
+ * block; cfg < 0 keeps one step per pass.  The autotuner chooses it per grid
+ * shape; this pins it. */
+int jxf_num_blocked_configs(void);
+int jxf_grid3d_set_blocked(jxf_grid3d* g, int32_t cfg, int32_t x_chunk);
 
 /* Relative permittivity, replaces _build_epsilon_r (fdtd3d.py:132-137) and
  * the per-cell factor (dt_eps_dx / eps_r) of fdtd3d.py:299,336,345,354.

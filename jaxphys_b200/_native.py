@@ -55,6 +55,8 @@ class Grid3DInfo(C.Structure):
         ("kernels_per_step", C.c_int32),
         ("shell_blocks", C.c_int32), ("interior_blocks", C.c_int32),
         ("tma_config", C.c_int32), ("axis_split", C.c_int32),
+        ("blocked_config", C.c_int32), ("blocked_x_chunk", C.c_int32),
+        ("blocked_kernels_per_pass", C.c_int32),
     ]
 
 
@@ -99,6 +101,8 @@ SIGNATURES = {
     "jxf_grid3d_get_info": (C.c_int, [_vp, C.POINTER(Grid3DInfo)]),
     "jxf_grid3d_set_launch": (C.c_int, [_vp, _i32, _i32]),
     "jxf_grid3d_set_axis_split": (C.c_int, [_vp, _i32]),
+    "jxf_num_blocked_configs": (C.c_int, []),
+    "jxf_grid3d_set_blocked": (C.c_int, [_vp, _i32, _i32]),
     "jxf_grid3d_set_eps_host": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_set_eps_device": (C.c_int, [_vp, _vp, _vp]),
     "jxf_grid3d_set_sources": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),

@@ -19,14 +19,15 @@ ROOT = HERE.parent
 CSRC = HERE / "csrc"
 OUT = HERE / "_lib" / "libjaxphys_fdtd.so"
 
-SOURCES = ["capi.cu"]
-HEADERS = ["fdtd_common.cuh", "fdtd3d_kernels.cuh", "fdtd3d_adjoint.cuh", "fdtd2d_kernels.cuh",
+SOURCES = ["capi.cu", "tb_kernels.cu"]
+HEADERS = ["fdtd_common.cuh", "fdtd3d_kernels.cuh", "fdtd3d_tb.cuh", "tb_registry.h",
+           "fdtd3d_adjoint.cuh", "fdtd2d_kernels.cuh",
            "tc_common.cuh", "learned_band.cuh", "viz_kernels.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -46,15 +47,32 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every source to an object in parallel, then link the shared
+    library (CUDA runtime linked statically)."""
     if not force and not needs_build():
         return OUT
     OUT.parent.mkdir(parents=True, exist_ok=True)
+    objs = []
+    procs = []
+    for src in SOURCES:
+        obj = OUT.parent / (Path(src).stem + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", "-o", str(obj), str(CSRC / src)]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((subprocess.Popen(cmd), cmd))
+        objs.append(obj)
+    for proc, cmd in procs:
+        if proc.wait() != 0:
+            raise subprocess.CalledProcessError(proc.returncode, cmd)
     tmp = OUT.with_suffix(".so.tmp")
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(tmp),
+           *[str(o) for o in objs]]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(tmp, OUT)
+    for o in objs:
+        o.unlink(missing_ok=True)
     return OUT
 
 

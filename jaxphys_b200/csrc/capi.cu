@@ -22,6 +22,7 @@
 #include "fdtd3d_adjoint.cuh"
 #include "fdtd3d_kernels.cuh"
 #include "learned_band.cuh"
+#include "tb_registry.h"
 #include "viz_kernels.cuh"
 
 using namespace jxf;
@@ -249,9 +250,10 @@ const std::vector<TmaConfig>& tma_configs() {
   return cfgs;
 }
 
-// autotune results: (nx, ny, nz, mode, cbarr) -> (cfg index, x_chunk, axis split)
+// autotune results: (nx, ny, nz, mode, cbarr) -> (cfg index, x_chunk, axis split,
+// blocked cfg index or -1, blocked x_chunk)
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, std::tuple<int, int, int>> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int>, std::tuple<int, int, int, int, int>> g_tune_cache;
 
 }  // namespace
 
@@ -344,6 +346,25 @@ struct jxf_grid3d {
   bool maps_ok = false;
   int maps_cfg = -1;  // config whose box shapes the maps were encoded with
   Maps3D maps[2];     // input set 0 / 1
+  // two-level temporally blocked launches (tb_registry.h): tb = registry
+  // index, or -1 for one step per launch
+  int tb = -1, tb_chunk = 0;
+  bool maps_tb_ok = false;
+  int maps_tb_cfg = -1;
+  MapsTB maps_tb[2];
+  std::vector<long long> probe_cell_h;  // host copies for the per-block probe lists
+  std::vector<int> probe_comp_h;
+  TbSrc* d_tb_src = nullptr;
+  int* d_tb_src_ptr = nullptr;
+  TbProbe* d_tb_probe = nullptr;
+  int* d_tb_probe_ptr = nullptr;
+  int tb_built_cfg = -1, tb_built_chunk = -1;
+  int* d_tb_shell = nullptr;
+  int* d_tb_shell_ax[3] = {};
+  int* d_tb_inner = nullptr;
+  int n_tb_shell = 0, n_tb_inner = 0;
+  int n_tb_shell_ax[3] = {0, 0, 0};
+  int tb_split_cfg = -1, tb_split_chunk = -1, tb_split_axes = -1;
 };
 
 namespace {
@@ -736,6 +757,300 @@ int launch_step(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaSt
   return JXF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// two-level temporally blocked launches (fdtd3d_tb.cuh)
+// ---------------------------------------------------------------------------
+
+int tb_ntiles_z(const jxf_grid3d* g) { return (g->d.nz + TB_TZ - 1) / TB_TZ; }
+int tb_ntiles_y(const jxf_grid3d* g, const TbConfig& c) { return (g->d.ny + c.ty - 1) / c.ty; }
+
+int encode_maps_tb(jxf_grid3d* g) {
+  const TbConfig& c = tb_configs()[g->tb];
+  const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
+  for (int s = 0; s < 2; ++s) {
+    for (int k = 0; k < 3; ++k) {
+      TRY(encode_map(&g->maps_tb[s].e[k], g->f[s][k], nx, ny, nz, TB_BW, c.nr + 1));
+      TRY(encode_map(&g->maps_tb[s].h[k], g->f[s][3 + k], nx, ny, nz, TB_BW, c.nr));
+    }
+    if (g->cb) {
+      TRY(encode_map(&g->maps_tb[s].cb, g->cb, nx, ny, nz, TB_BW, c.nr));
+    } else {
+      g->maps_tb[s].cb = g->maps_tb[s].e[0];  // unused
+    }
+  }
+  g->maps_tb_ok = true;
+  g->maps_tb_cfg = g->tb;
+  return JXF_OK;
+}
+
+// Per-block source and probe lists of the blocked kernel (CSR over blocks in
+// grid order, entries sorted by plane, list order kept inside a plane).  A
+// source enters every block whose region (tile plus the two-cell halo) and
+// level-1 planes hold its cell: level 1 (step n) adds it to every region
+// cell; level 2 (step n+1) only on the owner's tile.  A probe enters its
+// owner block only.
+int build_tb_lists(jxf_grid3d* g) {
+  const TbConfig& c = tb_configs()[g->tb];
+  const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz, chunk = g->tb_chunk;
+  const int ntz = tb_ntiles_z(g), nty = tb_ntiles_y(g, c), nch = (nx + chunk - 1) / chunk;
+  const int nblk = ntz * nty * nch;
+  struct Keyed {
+    int blk, x, order;
+    TbSrc e;
+  };
+  std::vector<Keyed> ks;
+  for (size_t i = 0; i < g->src_cell.size(); ++i) {
+    const long long cell = g->src_cell[i];
+    const int z = (int)(cell % nz);
+    const int y = (int)((cell / nz) % ny);
+    const int x = (int)(cell / ((long long)nz * ny));
+    for (int ch = std::max(0, x / chunk - 1); ch <= std::min(nch - 1, (x + 2) / chunk); ++ch) {
+      const int xb = ch * chunk, xe = std::min(xb + chunk, nx);
+      const int qs = std::max(xb - 2, 0), q1 = std::min(xe, nx - 1);
+      if (x < qs || x > q1) continue;
+      for (int ty = std::max(0, (y + 2) / c.ty - 2); ty <= std::min(nty - 1, (y + 2) / c.ty + 1);
+           ++ty) {
+        const int y0 = ty * c.ty;
+        if (y < y0 - 2 || y > y0 - 2 + c.nr - 1) continue;
+        for (int tz = std::max(0, (z + 2) / TB_TZ - 2);
+             tz <= std::min(ntz - 1, (z + 2) / TB_TZ + 1); ++tz) {
+          const int z0 = tz * TB_TZ;
+          if (z < z0 - 2 || z > z0 + 29) continue;
+          const bool tile = y >= y0 && y < y0 + c.ty && z >= z0 && z < z0 + TB_TZ;
+          TbSrc e{};
+          e.x = x;
+          e.off = (y - (y0 - 2)) * 32 + (z - (z0 - 2));
+          e.comp = g->src_comp[i];
+          e.wave = g->src_wave[i];
+          e.amp = g->src_amp[i];
+          e.lv = 1 | ((tile && x >= xb && x < xe) ? 2 : 0);
+          ks.push_back({(ch * nty + ty) * ntz + tz, x, (int)i, e});
+        }
+      }
+    }
+  }
+  std::stable_sort(ks.begin(), ks.end(), [](const Keyed& u, const Keyed& v) {
+    if (u.blk != v.blk) return u.blk < v.blk;
+    return u.x < v.x;
+  });
+  std::vector<int> ptr(nblk + 1, 0);
+  std::vector<TbSrc> ents;
+  ents.reserve(ks.size());
+  for (const Keyed& k : ks) {
+    ents.push_back(k.e);
+    ptr[k.blk + 1]++;
+  }
+  for (int b = 0; b < nblk; ++b) ptr[b + 1] += ptr[b];
+  TRY(upload(&g->d_tb_src, ents, &g->bytes));
+  TRY(upload(&g->d_tb_src_ptr, ptr, &g->bytes));
+
+  struct KeyedP {
+    int blk, x;
+    TbProbe e;
+  };
+  std::vector<KeyedP> kp;
+  for (size_t j = 0; j < g->probe_cell_h.size(); ++j) {
+    const long long cell = g->probe_cell_h[j];
+    const int z = (int)(cell % nz);
+    const int y = (int)((cell / nz) % ny);
+    const int x = (int)(cell / ((long long)nz * ny));
+    const int tz = z / TB_TZ, ty = y / c.ty, ch = x / chunk;
+    TbProbe e{};
+    e.x = x;
+    e.off = (y - (ty * c.ty - 2)) * 32 + (z - (tz * TB_TZ - 2));
+    e.comp = g->probe_comp_h[j];
+    e.slot = (int)j;
+    kp.push_back({(ch * nty + ty) * ntz + tz, x, e});
+  }
+  std::stable_sort(kp.begin(), kp.end(), [](const KeyedP& u, const KeyedP& v) {
+    if (u.blk != v.blk) return u.blk < v.blk;
+    return u.x < v.x;
+  });
+  std::vector<int> pptr(nblk + 1, 0);
+  std::vector<TbProbe> pents;
+  for (const KeyedP& k : kp) {
+    pents.push_back(k.e);
+    pptr[k.blk + 1]++;
+  }
+  for (int b = 0; b < nblk; ++b) pptr[b + 1] += pptr[b];
+  TRY(upload(&g->d_tb_probe, pents, &g->bytes));
+  TRY(upload(&g->d_tb_probe_ptr, pptr, &g->bytes));
+  g->tb_built_cfg = g->tb;
+  g->tb_built_chunk = chunk;
+  return JXF_OK;
+}
+
+// CPML grids: blocks whose region (tile, two-cell halo, level-1 planes)
+// touches the psi slabs of several axes, of one axis, or none.
+int build_tb_split(jxf_grid3d* g, int cfg, int chunk) {
+  if (g->tb_split_cfg == cfg && g->tb_split_chunk == chunk && g->tb_split_axes == g->axis_split)
+    return JXF_OK;
+  const TbConfig& c = tb_configs()[cfg];
+  const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
+  const int ntz = tb_ntiles_z(g), nty = tb_ntiles_y(g, c);
+  const int nch = (nx + chunk - 1) / chunk;
+  struct Blk {
+    int cost, tz, ty, ch;
+  };
+  std::vector<Blk> shell_b, axl_b[3];
+  std::vector<int> inner;
+  const bool axis_split = g->axis_split != 0;
+  for (int ch = 0; ch < nch; ++ch)
+    for (int ty = 0; ty < nty; ++ty)
+      for (int tz = 0; tz < ntz; ++tz) {
+        const int z0 = tz * TB_TZ, y0 = ty * c.ty, xb = ch * chunk;
+        const int xe = std::min(xb + chunk, nx);
+        const bool cz = range_clear(z0 - 2, z0 + 29, nz, g->P[2]);
+        const bool cy = range_clear(y0 - 2, y0 + c.nr - 3, ny, g->P[1]);
+        const bool cx = range_clear(std::max(xb - 2, 0), std::min(xe, nx - 1), nx, g->P[0]);
+        const int touched = (cx ? 0 : 1) + (cy ? 0 : 1) + (cz ? 0 : 1);
+        if (touched == 0) {
+          inner.push_back(tz);
+          inner.push_back(ty);
+          inner.push_back(ch);
+          continue;
+        }
+        int xs = 0;  // level-1 planes inside the x slab
+        for (int x = std::max(xb - 2, 0); x <= std::min(xe, nx - 1); ++x)
+          xs += in_slab(x, nx, g->P[0]) ? 1 : 0;
+        std::vector<Blk>* v = &shell_b;
+        if (touched == 1 && !g->kappa && axis_split) v = &axl_b[!cx ? 0 : (!cy ? 1 : 2)];
+        v->push_back({touched * 4096 + xs, tz, ty, ch});
+      }
+  auto flatten = [&](std::vector<Blk>& in, std::vector<int>& out) {
+    if (heavy_first_enabled())
+      std::stable_sort(in.begin(), in.end(),
+                       [](const Blk& u, const Blk& v) { return u.cost > v.cost; });
+    for (const Blk& b : in) {
+      out.push_back(b.tz);
+      out.push_back(b.ty);
+      out.push_back(b.ch);
+    }
+  };
+  std::vector<int> shell, axl[3];
+  flatten(shell_b, shell);
+  for (int a = 0; a < 3; ++a) flatten(axl_b[a], axl[a]);
+  TRY(upload(&g->d_tb_shell, shell, &g->bytes));
+  TRY(upload(&g->d_tb_inner, inner, &g->bytes));
+  for (int a = 0; a < 3; ++a) {
+    TRY(upload(&g->d_tb_shell_ax[a], axl[a], &g->bytes));
+    g->n_tb_shell_ax[a] = (int)axl[a].size() / 3;
+  }
+  g->n_tb_shell = (int)shell.size() / 3;
+  g->n_tb_inner = (int)inner.size() / 3;
+  g->tb_split_cfg = cfg;
+  g->tb_split_chunk = chunk;
+  g->tb_split_axes = g->axis_split;
+  return JXF_OK;
+}
+
+int launch_tb(jxf_grid3d* g, int cfg, int chunk, Step3D& p, const TbExtra& ex, int in_set,
+              cudaStream_t st, int list_count, bool plain = false, int axis = -1) {
+  if (!g->maps_tb_ok || g->maps_tb_cfg != cfg)
+    return fail(JXF_ERR_INVALID, "blocked tensor maps encoded for config %d, launching %d",
+                g->maps_tb_cfg, cfg);
+  const TbConfig& c = tb_configs()[cfg];
+  const bool cpml = g->mode == MODE_CPML && !plain;
+  const int ki = cpml ? (g->kappa ? 2 : 1) : 0;
+  TbKernel k = c.k[ki][g->cb ? 1 : 0];
+  size_t smem = c.smem[cpml ? 1 : 0];
+  if (cpml && axis >= 0) {
+    k = c.kax[axis][g->cb ? 1 : 0];
+    smem = c.smem_ax[axis];
+  }
+  {
+    static std::mutex mu;
+    static std::map<std::pair<TbKernel, int>, size_t> done;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& have = done[{k, g->d.device}];
+    if (have < smem) {
+      CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared));
+      have = smem;
+    }
+  }
+  p.x_chunk = chunk;
+  p.ntiles_z = tb_ntiles_z(g);
+  p.ntiles_y = tb_ntiles_y(g, c);
+  dim3 grid(p.ntiles_z, p.ntiles_y, (g->d.nx + chunk - 1) / chunk);
+  if (list_count >= 0) grid = dim3(list_count, 1, 1);
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = grid;
+  lc.blockDim = dim3(c.threads, 1, 1);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = g->use_pdl ? 1 : 0;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&lc, k, p, g->maps_tb[in_set], ex);
+  if (e != cudaSuccess && g->use_pdl) {
+    (void)cudaGetLastError();
+    g->use_pdl = false;
+    p.pdl = 0;
+    lc.numAttrs = 0;
+    e = cudaLaunchKernelEx(&lc, k, p, g->maps_tb[in_set], ex);
+  }
+  if (e != cudaSuccess)
+    return fail(JXF_ERR_CUDA, "blocked step kernel launch failed: %s", cudaGetErrorString(e));
+  return JXF_OK;
+}
+
+// Two leapfrog steps in one pass (per part for CPML grids, chained by
+// programmatic dependent launch as in launch_step).
+int launch_tb_step(jxf_grid3d* g, int cfg, int chunk, Step3D& p, const TbExtra& ex, int in_set,
+                   cudaStream_t st) {
+  p.pdl = g->use_pdl ? (PDL_WAIT_START | PDL_TRIGGER) : 0;
+  if (g->mode != MODE_CPML) {
+    p.blk_list = nullptr;
+    return launch_tb(g, cfg, chunk, p, ex, in_set, st, -1);
+  }
+  TRY(build_tb_split(g, cfg, chunk));
+  struct Part {
+    const int* list;
+    int n;
+    bool plain;
+    int axis;
+  };
+  const Part parts[5] = {{g->d_tb_shell, g->n_tb_shell, false, -1},
+                         {g->d_tb_shell_ax[0], g->n_tb_shell_ax[0], false, 0},
+                         {g->d_tb_shell_ax[1], g->n_tb_shell_ax[1], false, 1},
+                         {g->d_tb_shell_ax[2], g->n_tb_shell_ax[2], false, 2},
+                         {g->d_tb_inner, g->n_tb_inner, true, -1}};
+  bool first = true;
+  for (const Part& part : parts) {
+    if (part.n <= 0) continue;
+    Step3D q = p;
+    q.blk_list = part.list;
+    if (!first) {
+      q.probe_out = nullptr;
+      if (g->use_pdl) q.pdl = PDL_TRIGGER | PDL_WAIT_END;
+    }
+    TRY(launch_tb(g, cfg, chunk, q, ex, in_set, st, part.n, part.plain, part.axis));
+    first = false;
+  }
+  return JXF_OK;
+}
+
+TbExtra tb_extra(const jxf_grid3d* g, float* probe_mid) {
+  TbExtra ex{};
+  ex.src_ptr = g->src_cell.empty() ? nullptr : g->d_tb_src_ptr;
+  ex.src = g->d_tb_src;
+  ex.probe_ptr = g->n_probes > 0 ? g->d_tb_probe_ptr : nullptr;
+  ex.probe = g->d_tb_probe;
+  ex.probe_mid = probe_mid;
+  return ex;
+}
+
+int ensure_tb_ready(jxf_grid3d* g) {
+  if (g->tb < 0) return JXF_OK;
+  if (!g->maps_tb_ok || g->maps_tb_cfg != g->tb) TRY(encode_maps_tb(g));
+  if (g->tb_built_cfg != g->tb || g->tb_built_chunk != g->tb_chunk) TRY(build_tb_lists(g));
+  return JXF_OK;
+}
+
 int heuristic_tune(jxf_grid3d* g) {
   // Small grids: smaller tiles and chunks keep >= 2 waves of blocks.
   const long long cells = g->n;
@@ -764,9 +1079,19 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
       g->cfg = std::get<0>(it->second);
       g->x_chunk = std::get<1>(it->second);
       g->axis_split = std::get<2>(it->second);
+      g->tb = std::get<3>(it->second);
+      g->tb_chunk = std::get<4>(it->second);
       return JXF_OK;
     }
   }
+  // JXF_TB: "off" keeps one step per launch; "cfg,chunk[,split]" pins the
+  // two-level blocked launch shape
+  const char* tb_env = std::getenv("JXF_TB");
+  const bool tb_off = tb_env && std::strcmp(tb_env, "off") == 0;
+  int tfc = -1, tfk = -1, tfs = -1;
+  const bool tb_forced = tb_env && !tb_off &&
+                         std::sscanf(tb_env, "%d,%d,%d", &tfc, &tfk, &tfs) >= 2 && tfc >= 0 &&
+                         tfc < (int)tb_configs().size() && tfk >= 1;
   const char* env = std::getenv("JXF_AUTOTUNE");
   const bool enabled = !(env && env[0] == '0');
   // "cfg,chunk[,split]": pin the launch shape (split defaults to off)
@@ -777,10 +1102,20 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
     g->cfg = fc;
     g->x_chunk = fk;
     g->axis_split = split_env >= 0 ? split_env : (fs != 0 ? 1 : 0);
+    g->tb = tb_forced ? tfc : -1;
+    g->tb_chunk = tb_forced ? tfk : 0;
+    if (tb_forced && tfs >= 0) g->axis_split = tfs != 0 ? 1 : 0;
     return JXF_OK;
   }
-  if (!enabled || g->n < (1LL << 18)) {
+  if (tb_forced) {
     TRY(heuristic_tune(g));
+    g->tb = tfc;
+    g->tb_chunk = tfk;
+    if (tfs >= 0) g->axis_split = tfs != 0 ? 1 : 0;
+    if (split_env >= 0) g->axis_split = split_env;
+  } else if (!enabled || g->n < (1LL << 18)) {
+    TRY(heuristic_tune(g));
+    g->tb = -1;
     if (split_env >= 0) g->axis_split = split_env;
   } else {
     cudaEvent_t e0, e1;
@@ -830,18 +1165,65 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
         }
       }
     }
+    // two-level blocked launches: time per leapfrog step = launch time / 2
+    int btb = -1, btk = 0, bts = bs;
+    if (!tb_off) {
+      const int tchunks[] = {8, 16, 32, 64};
+      for (int sp = 0; sp < 2; ++sp) {
+        if (sp == 1 && !can_split) continue;
+        if (split_env >= 0 && sp != split_env) continue;
+        for (int ti = 0; ti < (int)tb_configs().size(); ++ti) {
+          for (int ch : tchunks) {
+            if (ch > g->d.nx && ch != 8) continue;
+            g->tb = ti;
+            g->tb_chunk = ch;
+            g->axis_split = sp;
+            TRY(encode_maps_tb(g));
+            Step3D p = base_params(g);
+            set_io(g, p, g->cur, 1 - g->cur);
+            p.blk_src_ptr = nullptr;
+            p.probe_out = nullptr;
+            p.step = 0;
+            p.err = g->d_err;
+            TbExtra ex{};
+            TRY(launch_tb_step(g, ti, ch, p, ex, g->cur, st));
+            const int reps = g->n >= (1LL << 25) ? 2 : (g->n >= (1LL << 21) ? 20 : 50);
+            float ms = 1e30f;
+            for (int trial = 0; trial < 2; ++trial) {
+              CUDA_TRY(cudaEventRecord(e0, st));
+              for (int r = 0; r < reps; ++r) TRY(launch_tb_step(g, ti, ch, p, ex, g->cur, st));
+              CUDA_TRY(cudaEventRecord(e1, st));
+              CUDA_TRY(cudaEventSynchronize(e1));
+              float t = 0;
+              CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+              ms = std::min(ms, t * 0.5f);  // two leapfrog steps per launch
+            }
+            if (ms < best) {
+              best = ms;
+              btb = ti;
+              btk = ch;
+              bts = sp;
+            }
+          }
+        }
+      }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     g->cfg = bc;
     g->x_chunk = bk;
-    g->axis_split = bs;
+    g->axis_split = btb >= 0 ? bts : bs;
+    g->tb = btb;
+    g->tb_chunk = btk;
     g->maps_ok = false;  // maps hold the boxes of the last trial, not of the winner
+    g->maps_tb_ok = false;
     g->built_cfg = -1;
+    g->tb_built_cfg = -1;
     // The trials wrote only the idle buffer set, which the next real step
     // overwrites before anything reads it.
   }
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = std::make_tuple(g->cfg, g->x_chunk, g->axis_split);
+  g_tune_cache[key] = std::make_tuple(g->cfg, g->x_chunk, g->axis_split, g->tb, g->tb_chunk);
   return JXF_OK;
 }
 
@@ -850,6 +1232,7 @@ int ensure_tma_ready(jxf_grid3d* g, cudaStream_t st) {
   if (!g->maps_ok) TRY(encode_maps(g));
   if (!g->src_cell.empty() && (g->built_cfg != g->cfg || g->built_chunk != g->x_chunk))
     TRY(build_tma_sources(g));
+  TRY(ensure_tb_ready(g));
   return JXF_OK;
 }
 
@@ -1073,6 +1456,13 @@ int jxf_grid3d_destroy(jxf_grid3d* g) {
   dfree(g->d_shell);
   for (int a = 0; a < 3; ++a) dfree(g->d_shell_ax[a]);
   dfree(g->d_inner);
+  dfree(g->d_tb_src);
+  dfree(g->d_tb_src_ptr);
+  dfree(g->d_tb_probe);
+  dfree(g->d_tb_probe_ptr);
+  dfree(g->d_tb_shell);
+  for (int a = 0; a < 3; ++a) dfree(g->d_tb_shell_ax[a]);
+  dfree(g->d_tb_inner);
   dfree(g->adj_ck);
   dfree(g->adj_sg);
   dfree(g->adj_l);
@@ -1108,6 +1498,17 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
   out->interior_blocks = g->n_inner;
   out->tma_config = g->path == JXF_PATH_TMA ? g->cfg : -1;
   out->axis_split = g->axis_split;
+  out->blocked_config = g->path == JXF_PATH_TMA ? g->tb : -1;
+  out->blocked_x_chunk = g->path == JXF_PATH_TMA && g->tb >= 0 ? g->tb_chunk : 0;
+  if (g->path == JXF_PATH_TMA && g->tb >= 0)
+    out->blocked_kernels_per_pass =
+        g->mode != MODE_CPML || g->tb_split_cfg < 0
+            ? 1
+            : (g->n_tb_shell > 0 ? 1 : 0) + (g->n_tb_inner > 0 ? 1 : 0) +
+                  (g->n_tb_shell_ax[0] > 0 ? 1 : 0) + (g->n_tb_shell_ax[1] > 0 ? 1 : 0) +
+                  (g->n_tb_shell_ax[2] > 0 ? 1 : 0);
+  else
+    out->blocked_kernels_per_pass = 0;
   if (g->path == JXF_PATH_GENERIC)
     out->kernels_per_step = 2 + (g->n_cells > 0 ? 1 : 0);
   else if (g->mode == MODE_CPML && g->split_cfg >= 0)
@@ -1133,6 +1534,22 @@ int jxf_grid3d_set_launch(jxf_grid3d* g, int32_t cfg, int32_t x_chunk) {
   return JXF_OK;
 }
 
+int jxf_num_blocked_configs(void) { return (int)tb_configs().size(); }
+
+int jxf_grid3d_set_blocked(jxf_grid3d* g, int32_t cfg, int32_t x_chunk) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (g->path != JXF_PATH_TMA) return fail(JXF_ERR_INVALID, "grid does not use the TMA path");
+  if (cfg >= (int)tb_configs().size()) return fail(JXF_ERR_INVALID, "blocked cfg out of range");
+  if (cfg >= 0 && x_chunk < 1) return fail(JXF_ERR_INVALID, "x_chunk must be >= 1");
+  if (g->cfg < 0) TRY(heuristic_tune(g));  // one-step shape for odd remainders
+  g->tb = cfg < 0 ? -1 : cfg;
+  g->tb_chunk = cfg < 0 ? 0 : x_chunk;
+  g->maps_tb_ok = false;
+  g->tb_built_cfg = -1;
+  g->tb_split_cfg = -1;
+  return JXF_OK;
+}
+
 int jxf_grid3d_set_axis_split(jxf_grid3d* g, int32_t on) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
   g->axis_split = on ? 1 : 0;
@@ -1153,6 +1570,7 @@ int jxf_grid3d_set_eps_host(jxf_grid3d* g, const double* eps_r) {
   if (!eps_r) {
     dfree(g->cb);
     g->maps_ok = false;
+    g->maps_tb_ok = false;
     return JXF_OK;
   }
   std::vector<float> cb((size_t)g->n);
@@ -1164,6 +1582,7 @@ int jxf_grid3d_set_eps_host(jxf_grid3d* g, const double* eps_r) {
   }
   TRY(upload(&g->cb, cb, &g->bytes));
   g->maps_ok = false;
+  g->maps_tb_ok = false;
   return JXF_OK;
 }
 
@@ -1176,6 +1595,7 @@ int jxf_grid3d_set_eps_device(jxf_grid3d* g, const float* eps_r, void* stream) {
   k_cb_from_eps<<<592, 256, 0, (cudaStream_t)stream>>>(eps_r, g->cb, (float)g->coef_e, g->n);
   CUDA_TRY(cudaGetLastError());
   g->maps_ok = false;
+  g->maps_tb_ok = false;
   return JXF_OK;
 }
 
@@ -1196,6 +1616,7 @@ int jxf_grid3d_set_sources(jxf_grid3d* g, int32_t n, const int64_t* cell, const 
   g->src_wave.assign(wave_id, wave_id + n);
   TRY(build_generic_sources(g));
   g->built_cfg = -1;
+  g->tb_built_cfg = -1;
   return JXF_OK;
 }
 
@@ -1225,6 +1646,9 @@ int jxf_grid3d_set_probes(jxf_grid3d* g, int32_t n, const int64_t* cell, const i
   TRY(upload(&g->d_probe_cell, c, &g->bytes));
   TRY(upload(&g->d_probe_comp, k, &g->bytes));
   g->n_probes = n;
+  g->probe_cell_h = c;
+  g->probe_comp_h = k;
+  g->tb_built_cfg = -1;
   return JXF_OK;
 }
 
@@ -1261,13 +1685,24 @@ int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stre
     TRY(ensure_tma_ready(g, st));
     p.blk_src_ptr = g->src_cell.empty() ? nullptr : g->d_blk_ptr;
     p.src = g->d_entries;
-    for (int k = 0; k < n_steps; ++k) {
+    for (int k = 0; k < n_steps;) {
       set_io(g, p, g->cur, 1 - g->cur);
       p.step = g->step;
       p.probe_out = (probe_out && np > 0 && k >= 1) ? probe_out + (size_t)(k - 1) * np : nullptr;
+      if (g->tb >= 0 && n_steps - k >= 2) {
+        // two steps in one pass; the state after the first is recorded by
+        // the probe cells' owner blocks
+        const TbExtra ex = tb_extra(g, (probe_out && np > 0) ? probe_out + (size_t)k * np : nullptr);
+        TRY(launch_tb_step(g, g->tb, g->tb_chunk, p, ex, g->cur, st));
+        g->cur ^= 1;
+        g->step += 2;
+        k += 2;
+        continue;
+      }
       TRY(launch_step(g, g->cfg, g->x_chunk, p, g->cur, st));
       g->cur ^= 1;
       g->step++;
+      ++k;
     }
     if (probe_out && np > 0) TRY(gather_probes(g, g->cur, probe_out + (size_t)(n_steps - 1) * np, st));
   } else {

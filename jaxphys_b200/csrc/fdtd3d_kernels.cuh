@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256) k3d_batch_e(const __grid_constant__ Batch
 }
 
 // Soft sources, grouped by cell (list order within a cell), after the E update.
-__global__ void k3d_sources(float* ex, float* ey, float* ez, const SrcCell* cells, int n_cells,
+static __global__ void k3d_sources(float* ex, float* ey, float* ez, const SrcCell* cells, int n_cells,
                             const SrcTerm* terms, const float* wave, long long wave_len,
                             long long step) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -364,7 +364,7 @@ struct BatchSrcGrid {
   const float* wave;
   long long wave_len;
 };
-__global__ void k3d_batch_sources(const BatchSrcGrid* grids, const int2* entries, int n,
+static __global__ void k3d_batch_sources(const BatchSrcGrid* grids, const int2* entries, int n,
                                   long long step) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -385,7 +385,7 @@ struct BatchProbe {
   int grid, comp;
   long long cell;
 };
-__global__ void k3d_batch_probes(const Step3D* grids, const BatchProbe* pr, int n, float* out) {
+static __global__ void k3d_batch_probes(const Step3D* grids, const BatchProbe* pr, int n, float* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const BatchProbe q = pr[i];
@@ -397,7 +397,7 @@ struct FieldPtrs6 {
 };
 
 // probe_out[i] = field[comp_i][cell_i]
-__global__ void k_probe_gather(FieldPtrs6 fp, const long long* cell, const int* comp, int n,
+static __global__ void k_probe_gather(FieldPtrs6 fp, const long long* cell, const int* comp, int n,
                                float* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = fp.f[comp[i]][cell[i]];
