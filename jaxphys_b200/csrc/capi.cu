@@ -80,10 +80,17 @@ struct DeviceGuard {
   }
 };
 
+// Fault injection for the failure-detection tests: JXF_FAULT_ALLOC_AFTER=n
+// (read when a grid is created) lets the next n device allocations of that
+// creation succeed and fails the one after with JXF_ERR_OOM.
+thread_local long long g_alloc_budget = -1;
+
 template <class T>
 int dmalloc(T** p, size_t count, int64_t* tally) {
   *p = nullptr;
   if (count == 0) return JXF_OK;
+  if (g_alloc_budget == 0) return fail(JXF_ERR_OOM, "device allocation refused (fault injection)");
+  if (g_alloc_budget > 0) --g_alloc_budget;
   CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T)));
   *tally += (int64_t)(count * sizeof(T));
   return JXF_OK;
@@ -480,8 +487,20 @@ unsigned long long wait_limit_ns() {
   return v;
 }
 
+// Fault injection for the failure-detection tests, read at every step call:
+// JXF_FAULT_DROP_STAGE=l makes every block of the TMA step kernels skip the
+// copy of its l-th staged plane (its bounded waits then run out and the step
+// reports JXF_ERR_TIMEOUT through jxf_grid3d_check_error).
+int fault_drop_stage() {
+  const char* e = std::getenv("JXF_FAULT_DROP_STAGE");
+  if (!e || !*e) return -1;
+  const int v = std::atoi(e);
+  return v >= 0 ? v : -1;
+}
+
 Step3D base_params(jxf_grid3d* g) {
   Step3D p{};
+  p.drop_stage = fault_drop_stage();
   p.nx = g->d.nx;
   p.ny = g->d.ny;
   p.nz = g->d.nz;
@@ -1303,8 +1322,20 @@ int jxf_grid3d_create_slab(const jxf_grid3d_desc* desc, int32_t x0, int32_t x1,
   return create3d(d, desc->nx, x0 - 1, 1, x1 - x0 + 1, true, out);
 }
 
+static int create3d_impl(const jxf_grid3d_desc& d, int gnx, int gx0, int x_lo, int x_hi,
+                         bool slab, jxf_grid3d** out);
+
 static int create3d(const jxf_grid3d_desc& d, int gnx, int gx0, int x_lo, int x_hi, bool slab,
                     jxf_grid3d** out) {
+  const char* e = std::getenv("JXF_FAULT_ALLOC_AFTER");
+  g_alloc_budget = (e && *e) ? std::max(0LL, std::atoll(e)) : -1;
+  const int rc = create3d_impl(d, gnx, gx0, x_lo, x_hi, slab, out);
+  g_alloc_budget = -1;
+  return rc;
+}
+
+static int create3d_impl(const jxf_grid3d_desc& d, int gnx, int gx0, int x_lo, int x_hi,
+                         bool slab, jxf_grid3d** out) {
   if (d.nx < 2 || d.ny < 2 || d.nz < 2)
     return fail(JXF_ERR_INVALID, "grid must be at least 2 cells per axis, got %dx%dx%d", d.nx, d.ny,
                 d.nz);
@@ -3384,6 +3415,7 @@ extern "C" int jxf_grid3d_run_noalloc(const jxf_noalloc_desc* desc, float* const
     }
   }
   Step3D p{};
+  p.drop_stage = -1;
   p.nx = d.nx;
   p.ny = d.ny;
   p.nz = d.nz;

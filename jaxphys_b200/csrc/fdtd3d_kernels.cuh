@@ -638,6 +638,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   __syncthreads();
 
   auto issue = [&](int l) {
+    if (l == p.drop_stage) return;  // fault injection: this stage never arrives
     const int slot = l % STAGES;
     float* st = stages + slot * L::STAGE_FLOATS;
     const int q = qs + l;

@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(32 * NW)
   __syncthreads();
 
   auto issue = [&](int l) {
+    if (l == p.drop_stage) return;  // fault injection: this stage never arrives
     const int slot = l % STAGES;
     float* st = stages + slot * L::STAGE_FLOATS;
     const int q = qs + l;

@@ -135,6 +135,10 @@ struct Step3D {
   // index decode of the generic kernels (idx32: every local index < 2^32)
   FastDiv div_nz, div_ny;
   int idx32;
+  // fault injection for the failure-detection tests: every block of the TMA
+  // kernels leaves the copy of its staged plane with this index unissued, so
+  // its bounded waits run out (-1: off; set from JXF_FAULT_DROP_STAGE)
+  int drop_stage;
 };
 
 enum PdlBits : int { PDL_WAIT_START = 1, PDL_TRIGGER = 2, PDL_WAIT_END = 4 };
