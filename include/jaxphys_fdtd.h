@@ -203,6 +203,12 @@ int jxf_batch3d_destroy(jxf_batch3d* b);
 int jxf_batch3d_reset(jxf_batch3d* b, void* stream);
 int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_graph, void* stream);
 int jxf_batch3d_probes(jxf_batch3d* b, int32_t grid, int32_t n_steps, float* dst, void* stream);
+/* Kernel launches per leapfrog step of the batch's current shape, and the
+ * launch shape of a TMA batch (registry entry, x chunk, single-axis split;
+ * -1 each for a generic batch).  No reference counterpart (the reference runs
+ * one grid per simulate() call, fdtd3d.py:169). */
+int jxf_batch3d_kernels_per_step(const jxf_batch3d* b);
+int jxf_batch3d_launch(const jxf_batch3d* b, int32_t* out3);
 
 /* Learned absorbing band (extension; the reference has only the graded PML).
  * A jxf_band holds one small network per face of a box (6 faces,

@@ -102,6 +102,8 @@ SIGNATURES = {
     "jxf_grid3d_set_launch": (C.c_int, [_vp, _i32, _i32]),
     "jxf_grid3d_set_axis_split": (C.c_int, [_vp, _i32]),
     "jxf_num_blocked_configs": (C.c_int, []),
+    "jxf_batch3d_kernels_per_step": (C.c_int, [_vp]),
+    "jxf_batch3d_launch": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "jxf_grid3d_set_blocked": (C.c_int, [_vp, _i32, _i32]),
     "jxf_grid3d_set_eps_host": (C.c_int, [_vp, _vp]),
     "jxf_grid3d_set_eps_device": (C.c_int, [_vp, _vp, _vp]),

@@ -19,8 +19,9 @@ ROOT = HERE.parent
 CSRC = HERE / "csrc"
 OUT = HERE / "_lib" / "libjaxphys_fdtd.so"
 
-SOURCES = ["capi.cu", "tb_kernels.cu"]
+SOURCES = ["capi.cu", "tma_kernels.cu", "tb_kernels.cu"]
 HEADERS = ["fdtd_common.cuh", "fdtd3d_kernels.cuh", "fdtd3d_tb.cuh", "tb_registry.h",
+           "tma_registry.h",
            "fdtd3d_adjoint.cuh", "fdtd2d_kernels.cuh",
            "tc_common.cuh", "learned_band.cuh", "viz_kernels.cuh"]
 

@@ -23,6 +23,7 @@
 #include "fdtd3d_kernels.cuh"
 #include "learned_band.cuh"
 #include "tb_registry.h"
+#include "tma_registry.h"
 #include "viz_kernels.cuh"
 
 using namespace jxf;
@@ -204,59 +205,6 @@ int encode_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, int bz
 // TMA kernel registry
 // ---------------------------------------------------------------------------
 
-using TmaKernel = void (*)(const Step3D, const Maps3D);
-
-struct TmaConfig {
-  int tz, ty, ry, stages;
-  int threads;
-  size_t smem[2];     // [mode: 0 absorb, 1 cpml]
-  TmaKernel k[3][2];  // [0 absorb, 1 cpml (kappa = 1), 2 cpml (kappa > 1)][cbarr]
-  // CPML (kappa = 1) for blocks touching the slab of one axis only [x, y, z][cbarr]
-  size_t smem_ax[3];
-  TmaKernel kax[3][2];
-};
-
-template <int TZ, int TY, int RY, int ST>
-TmaConfig make_cfg() {
-  TmaConfig c;
-  c.tz = TZ;
-  c.ty = TY;
-  c.ry = RY;
-  c.stages = ST;
-  c.threads = TZ * (TY / RY);
-  c.smem[0] = TmaLayout<TZ, TY, RY, ST, true, false>::SMEM_BYTES;
-  c.smem[1] = TmaLayout<TZ, TY, RY, ST, true, true>::SMEM_BYTES;
-  c.k[0][0] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, false, false>;
-  c.k[0][1] = k3d_tma<TZ, TY, RY, ST, MODE_ABSORB, true, false>;
-  c.k[1][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false>;
-  c.k[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false>;
-  c.k[2][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, true>;
-  c.k[2][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, true>;
-  c.smem_ax[0] = TmaLayout<TZ, TY, RY, ST, true, true, 1>::SMEM_BYTES;
-  c.smem_ax[1] = TmaLayout<TZ, TY, RY, ST, true, true, 2>::SMEM_BYTES;
-  c.smem_ax[2] = TmaLayout<TZ, TY, RY, ST, true, true, 4>::SMEM_BYTES;
-  c.kax[0][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 1>;
-  c.kax[0][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 1>;
-  c.kax[1][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 2>;
-  c.kax[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 2>;
-  c.kax[2][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 4>;
-  c.kax[2][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 4>;
-  return c;
-}
-
-const std::vector<TmaConfig>& tma_configs() {
-  static const std::vector<TmaConfig> cfgs = {
-      make_cfg<32, 8, 1, 4>(),  make_cfg<32, 16, 2, 4>(), make_cfg<64, 8, 2, 3>(),
-      make_cfg<32, 16, 4, 4>(), make_cfg<64, 16, 4, 3>(),
-      // small-grid shapes: 128-thread blocks (more blocks per SM, less
-      // shared memory per block), 3-stage ring
-      make_cfg<32, 4, 1, 4>(),  make_cfg<32, 8, 2, 4>(),  make_cfg<32, 8, 1, 3>(),
-      make_cfg<64, 4, 1, 3>(),  make_cfg<32, 4, 1, 3>(),  make_cfg<16, 8, 1, 3>(),
-      make_cfg<64, 8, 1, 3>(),
-  };
-  return cfgs;
-}
-
 // autotune results: (nx, ny, nz, mode, cbarr) -> (cfg index, x_chunk, axis split,
 // blocked cfg index or -1, blocked x_chunk)
 std::mutex g_tune_mu;
@@ -273,7 +221,8 @@ std::map<std::tuple<int, int, int, int, int>, std::tuple<int, int, int, int, int
 // each tile and the correction buffer.
 struct BandTables {
   jxf_band* band = nullptr;
-  band::GridRef* d_grids = nullptr;
+  band::GridRef* d_grids = nullptr;    // fields of buffer set 0 of every grid
+  band::GridRef* d_grids_b = nullptr;  // set 1 (TMA grids ping-pong; = set 0 otherwise)
   int2* d_cells = nullptr;
   int* d_tile_face = nullptr;
   float* d_delta = nullptr;
@@ -282,7 +231,7 @@ struct BandTables {
 };
 
 namespace {
-int band_launch(const BandTables& t, cudaStream_t st);
+int band_launch(const BandTables& t, cudaStream_t st, int set = 0);
 void band_release(BandTables& t);
 }  // namespace
 
@@ -670,9 +619,15 @@ double shell_block_cost(const jxf_grid3d* g, const TmaConfig& c, int cw, int xb,
   return cost;
 }
 
-int build_split(jxf_grid3d* g, int cfg, int chunk) {
-  if (g->split_cfg == cfg && g->split_chunk == chunk && g->split_axes == g->axis_split)
-    return JXF_OK;
+// Block lists of a CPML grid at one launch shape: shell blocks that touch the
+// slabs of several axes, of one axis (x, y, z), and interior blocks, each as
+// (tile_z, tile_y, chunk word) triples with a work estimate, heaviest first.
+struct SplitLists {
+  std::vector<int> list[5];     // [0 shell, 1..3 single-axis x/y/z, 4 interior]
+  std::vector<double> cost[5];  // per block
+};
+
+void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, SplitLists& out) {
   const TmaConfig& c = tma_configs()[cfg];
   const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
   const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
@@ -681,10 +636,9 @@ int build_split(jxf_grid3d* g, int cfg, int chunk) {
     double cost;
     int tz, ty, word;
   };
-  std::vector<Blk> shell_b, axl_b[3];
+  std::vector<Blk> parts[5];
   std::vector<int> tile_cw((size_t)ntz * nty, -1);  // filled on first use
-  std::vector<int> shell, inner, axl[3];
-  const bool axis_split = g->axis_split != 0;
+  const int warps = (c.threads + 31) / 32;
   for (int ch = 0; ch < nch; ++ch)
     for (int ty = 0; ty < nty; ++ty)
       for (int tz = 0; tz < ntz; ++tz) {
@@ -696,40 +650,46 @@ int build_split(jxf_grid3d* g, int cfg, int chunk) {
         const bool cx = range_clear(xb - 1, xe - 1, nx, g->P[0]);
         const int touched = (cx ? 0 : 1) + (cy ? 0 : 1) + (cz ? 0 : 1);
         if (touched == 0) {
-          inner.push_back(tz);
-          inner.push_back(ty);
-          inner.push_back(ch);
+          parts[4].push_back({(double)(xe - std::max(xb - 1, 0)) * warps, tz, ty, ch});
           continue;
         }
-        std::vector<Blk>* v = &shell_b;
-        if (touched == 1 && !g->kappa && axis_split) v = &axl_b[!cx ? 0 : (!cy ? 1 : 2)];
+        int pi = 0;
+        if (touched == 1 && !g->kappa && axis_split) pi = 1 + (!cx ? 0 : (!cy ? 1 : 2));
         // blocks holding z-slab cells order them first (one row per thread)
         const bool slab_first = !cz && c.ry == 1 && slab_first_enabled();
         int& cw = tile_cw[(size_t)ty * ntz + tz];
         if (cw < 0) cw = tile_cpml_warps(g, c, z0, y0, slab_first);
-        v->push_back({shell_block_cost(g, c, cw, xb, xe), tz, ty,
-                      ch | (slab_first ? BLK_SLAB_FIRST : 0)});
+        parts[pi].push_back({shell_block_cost(g, c, cw, xb, xe), tz, ty,
+                             ch | (slab_first ? BLK_SLAB_FIRST : 0)});
       }
-  auto flatten = [&](std::vector<Blk>& in, std::vector<int>& out) {
-    if (heavy_first_enabled())
-      std::stable_sort(in.begin(), in.end(),
+  for (int k = 0; k < 5; ++k) {
+    if (k < 4 && heavy_first_enabled())
+      std::stable_sort(parts[k].begin(), parts[k].end(),
                        [](const Blk& u, const Blk& v) { return u.cost > v.cost; });
-    for (const Blk& b : in) {
-      out.push_back(b.tz);
-      out.push_back(b.ty);
-      out.push_back(b.word);
+    out.list[k].clear();
+    out.cost[k].clear();
+    for (const Blk& b : parts[k]) {
+      out.list[k].push_back(b.tz);
+      out.list[k].push_back(b.ty);
+      out.list[k].push_back(b.word);
+      out.cost[k].push_back(b.cost);
     }
-  };
-  flatten(shell_b, shell);
-  for (int a = 0; a < 3; ++a) flatten(axl_b[a], axl[a]);
-  TRY(upload(&g->d_shell, shell, &g->bytes));
-  TRY(upload(&g->d_inner, inner, &g->bytes));
-  for (int a = 0; a < 3; ++a) {
-    TRY(upload(&g->d_shell_ax[a], axl[a], &g->bytes));
-    g->n_shell_ax[a] = (int)axl[a].size() / 3;
   }
-  g->n_shell = (int)shell.size() / 3;
-  g->n_inner = (int)inner.size() / 3;
+}
+
+int build_split(jxf_grid3d* g, int cfg, int chunk) {
+  if (g->split_cfg == cfg && g->split_chunk == chunk && g->split_axes == g->axis_split)
+    return JXF_OK;
+  SplitLists sl;
+  compute_split(g, cfg, chunk, g->axis_split != 0, sl);
+  TRY(upload(&g->d_shell, sl.list[0], &g->bytes));
+  TRY(upload(&g->d_inner, sl.list[4], &g->bytes));
+  for (int a = 0; a < 3; ++a) {
+    TRY(upload(&g->d_shell_ax[a], sl.list[1 + a], &g->bytes));
+    g->n_shell_ax[a] = (int)sl.list[1 + a].size() / 3;
+  }
+  g->n_shell = (int)sl.list[0].size() / 3;
+  g->n_inner = (int)sl.list[4].size() / 3;
   g->split_cfg = cfg;
   g->split_chunk = chunk;
   g->split_axes = g->axis_split;
@@ -1173,7 +1133,7 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
             CUDA_TRY(cudaEventSynchronize(e1));
             float t = 0;
             CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
-            ms = std::min(ms, t);
+            ms = std::min(ms, t / (float)reps);  // per leapfrog step
           }
           if (ms < best) {
             best = ms;
@@ -1215,7 +1175,7 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
               CUDA_TRY(cudaEventSynchronize(e1));
               float t = 0;
               CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
-              ms = std::min(ms, t * 0.5f);  // two leapfrog steps per launch
+              ms = std::min(ms, t / (2.0f * (float)reps));  // two leapfrog steps per launch
             }
             if (ms < best) {
               best = ms;
@@ -2223,11 +2183,235 @@ struct jxf_batch3d {
   int graph_n = -1;
   size_t cap[7] = {0, 0, 0, 0, 0, 0, 0};  // element capacity of the uploaded tables
   BandTables band;  // learned absorbing band (PEC batches only)
+  // TMA batches (every member grid on the TMA path): one persistent launch
+  // per step and CPML part over a work list of every grid's blocks
+  bool tma = false;
+  int cfg = -1, chunk = 0, axis_split = 0;
+  bool cbarr = false, kappa = false, use_pdl = true;
+  Step3D* d_tparams = nullptr;  // [2][n]: input set 0 / 1
+  Maps3D* d_tmaps = nullptr;    // [2][n]
+  int4* d_items = nullptr;      // parts concatenated
+  int* d_counters = nullptr;    // [5][2]
+  int part_off[5] = {0, 0, 0, 0, 0}, part_n[5] = {0, 0, 0, 0, 0}, part_ctas[5] = {0, 0, 0, 0, 0};
+  size_t tcap[3] = {0, 0, 0};
+  int graph_set = -1;           // input set at the start of the captured run
+  bool tuned = false;
 };
 
 namespace {
 
+// Dynamic shared-memory opt-in of a kernel, set once per kernel and device.
+int tma_smem_optin(const void* k, size_t smem, int device) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& have = done[{k, device}];
+  if (have < smem) {
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    have = smem;
+  }
+  return JXF_OK;
+}
+
+// Persistent batch kernel and its shared memory for a part (0 shell, 1..3
+// single-axis x / y / z shell, 4 interior; non-CPML batches use part 4).
+void batch_tma_kernel(const jxf_batch3d* b, int part, TmaBatchKernel* k, size_t* smem) {
+  const TmaConfig& c = tma_configs()[b->cfg];
+  const int cb = b->cbarr ? 1 : 0;
+  if (b->mode != MODE_CPML || part == 4) {
+    *k = c.kb[0][cb];
+    *smem = c.smem[0];
+  } else if (part == 0) {
+    *k = c.kb[b->kappa ? 2 : 1][cb];
+    *smem = c.smem[1];
+  } else {
+    *k = c.kbax[part - 1][cb];
+    *smem = c.smem_ax[part - 1];
+  }
+}
+
+// One leapfrog step of a TMA batch: the parts' persistent launches chained by
+// programmatic dependent launch (capturable).
+int batch_tma_launch(jxf_batch3d* b, int in_set, cudaStream_t st) {
+  const TmaConfig& c = tma_configs()[b->cfg];
+  bool first = true;
+  for (int pi = 0; pi < 5; ++pi) {
+    if (b->part_n[pi] == 0) continue;
+    TmaBatchKernel k;
+    size_t smem;
+    batch_tma_kernel(b, pi, &k, &smem);
+    TmaBatchArgs a{};
+    a.params = b->d_tparams;
+    a.maps = b->d_tmaps;
+    a.n_grids = (int)b->grids.size();
+    a.in_set = in_set;
+    a.items = b->d_items + b->part_off[pi];
+    a.n_items = b->part_n[pi];
+    a.counter = b->d_counters + 2 * pi;
+    a.pdl = b->use_pdl ? (first ? (PDL_WAIT_START | PDL_TRIGGER) : (PDL_TRIGGER | PDL_WAIT_END))
+                       : 0;
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(b->part_ctas[pi], 1, 1);
+    lc.blockDim = dim3(c.threads, 1, 1);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = b->use_pdl ? 1 : 0;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&lc, k, a);
+    if (e != cudaSuccess)
+      return fail(JXF_ERR_CUDA, "batch step kernel launch failed: %s", cudaGetErrorString(e));
+    first = false;
+  }
+  return JXF_OK;
+}
+
+// Launch tables of a TMA batch at its launch shape (b->cfg, b->chunk,
+// b->axis_split): per-grid parameters and tensor maps for both input sets,
+// per-block source lists, and the work items of every part (shell, x / y / z
+// single-axis shell, interior for CPML; one part otherwise), each part's
+// items heaviest first across all grids.  Buffers keep their addresses when
+// large enough (a captured graph holds them); any reallocation drops the graph.
+int batch_tma_tables(jxf_batch3d* b, bool* moved) {
+  const int n = (int)b->grids.size();
+  const TmaConfig& c = tma_configs()[b->cfg];
+  std::vector<Step3D> params(2 * (size_t)n);
+  std::vector<Maps3D> maps(2 * (size_t)n);
+  struct Item {
+    double cost;
+    int4 w;
+  };
+  std::vector<Item> parts[5];
+  const int warps = (c.threads + 31) / 32;
+  for (int k = 0; k < n; ++k) {
+    jxf_grid3d* g = b->grids[k];
+    if (g->cfg != b->cfg || g->x_chunk != b->chunk) {
+      g->cfg = b->cfg;
+      g->x_chunk = b->chunk;
+      g->maps_ok = false;
+      g->built_cfg = -1;
+    }
+    g->axis_split = b->axis_split;
+    g->tb = -1;
+    if (!g->maps_ok || g->maps_cfg != g->cfg) TRY(encode_maps(g));
+    if (!g->src_cell.empty() && (g->built_cfg != g->cfg || g->built_chunk != g->x_chunk))
+      TRY(build_tma_sources(g));
+    for (int s = 0; s < 2; ++s) {
+      Step3D p = base_params(g);
+      set_io(g, p, s, 1 - s);
+      p.blk_src_ptr = g->src_cell.empty() ? nullptr : g->d_blk_ptr;
+      p.src = g->d_entries;
+      p.probe_out = nullptr;
+      p.blk_list = nullptr;
+      p.pdl = 0;
+      p.x_chunk = b->chunk;
+      p.ntiles_z = (g->d.nz + c.tz - 1) / c.tz;
+      p.ntiles_y = (g->d.ny + c.ty - 1) / c.ty;
+      params[(size_t)s * n + k] = p;
+      maps[(size_t)s * n + k] = g->maps[s];
+    }
+    if (b->mode == MODE_CPML) {
+      SplitLists sl;
+      compute_split(g, b->cfg, b->chunk, b->axis_split != 0, sl);
+      for (int pi = 0; pi < 5; ++pi)
+        for (size_t i = 0; i < sl.cost[pi].size(); ++i)
+          parts[pi].push_back({sl.cost[pi][i], make_int4(k, sl.list[pi][3 * i],
+                                                         sl.list[pi][3 * i + 1],
+                                                         sl.list[pi][3 * i + 2])});
+    } else {
+      const int ntz = (g->d.nz + c.tz - 1) / c.tz, nty = (g->d.ny + c.ty - 1) / c.ty;
+      const int nch = (g->d.nx + b->chunk - 1) / b->chunk;
+      for (int ch = 0; ch < nch; ++ch) {
+        const int xb = ch * b->chunk, xe = std::min(xb + b->chunk, g->d.nx);
+        const double cost = (double)(xe - std::max(xb - 1, 0)) * warps;
+        for (int ty = 0; ty < nty; ++ty)
+          for (int tz = 0; tz < ntz; ++tz) parts[4].push_back({cost, make_int4(k, tz, ty, ch)});
+      }
+    }
+  }
+  std::vector<int4> items;
+  for (int pi = 0; pi < 5; ++pi) {
+    std::stable_sort(parts[pi].begin(), parts[pi].end(),
+                     [](const Item& u, const Item& v) { return u.cost > v.cost; });
+    b->part_off[pi] = (int)items.size();
+    b->part_n[pi] = (int)parts[pi].size();
+    for (const Item& it : parts[pi]) items.push_back(it.w);
+  }
+  auto put = [&](auto** ptr, size_t* cap, const auto& v) -> int {
+    if (v.empty()) return JXF_OK;
+    if (*cap < v.size()) {
+      dfree(*ptr);
+      TRY(dmalloc(ptr, v.size(), &b->bytes));
+      *cap = v.size();
+      *moved = true;
+    }
+    CUDA_TRY(cudaMemcpy(*ptr, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice));
+    return JXF_OK;
+  };
+  TRY(put(&b->d_tparams, &b->tcap[0], params));
+  TRY(put(&b->d_tmaps, &b->tcap[1], maps));
+  TRY(put(&b->d_items, &b->tcap[2], items));
+  if (!b->d_counters) {
+    TRY(dmalloc(&b->d_counters, 10, &b->bytes));
+    CUDA_TRY(cudaMemset(b->d_counters, 0, 10 * sizeof(int)));
+    *moved = true;
+  }
+  // persistent CTAs per part: resident blocks per SM times the SM count
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  for (int pi = 0; pi < 5; ++pi) {
+    b->part_ctas[pi] = 0;
+    if (b->part_n[pi] == 0) continue;
+    TmaBatchKernel k;
+    size_t smem;
+    batch_tma_kernel(b, pi, &k, &smem);
+    TRY(tma_smem_optin(reinterpret_cast<const void*>(k), smem, b->device));
+    int per_sm = 1;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, c.threads, smem));
+    b->part_ctas[pi] = std::max(1, std::min(b->part_n[pi], std::max(per_sm, 1) * sms));
+  }
+  return JXF_OK;
+}
+
+int batch_refresh_tma(jxf_batch3d* b) {
+  std::vector<BatchProbe> pr;
+  b->probe_offset.clear();
+  for (size_t k = 0; k < b->grids.size(); ++k) {
+    jxf_grid3d* g = b->grids[k];
+    b->probe_offset.push_back((int)pr.size());
+    for (int i = 0; i < g->n_probes; ++i)
+      pr.push_back(BatchProbe{(int)k, g->probe_comp_h[i], g->probe_cell_h[i]});
+  }
+  const int old_items = b->part_off[4] + b->part_n[4];
+  int old_ctas[5];
+  for (int i = 0; i < 5; ++i) old_ctas[i] = b->part_ctas[i];
+  bool moved = false;
+  TRY(batch_tma_tables(b, &moved));
+  bool shape = b->n_probes != (int)pr.size() || old_items != b->part_off[4] + b->part_n[4];
+  for (int i = 0; i < 5; ++i) shape = shape || old_ctas[i] != b->part_ctas[i];
+  b->n_probes = (int)pr.size();
+  if (!pr.empty() && b->cap[6] < pr.size()) {
+    dfree(b->d_probes);
+    TRY(dmalloc(&b->d_probes, pr.size(), &b->bytes));
+    b->cap[6] = pr.size();
+    moved = true;
+  }
+  if (!pr.empty())
+    CUDA_TRY(cudaMemcpy(b->d_probes, pr.data(), pr.size() * sizeof(BatchProbe),
+                        cudaMemcpyHostToDevice));
+  if ((moved || shape) && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return JXF_OK;
+}
+
 int batch_refresh(jxf_batch3d* b) {
+  if (b->tma) return batch_refresh_tma(b);
   // parameters, block tables, sources and probes of every grid (cheap; done
   // per call so later set_eps / set_sources on the member grids are seen)
   std::vector<Step3D> params;
@@ -2302,8 +2486,20 @@ int batch_refresh(jxf_batch3d* b) {
   return JXF_OK;
 }
 
-// One leapfrog step of every grid (kernels only; capturable).
-int batch_launch_step(jxf_batch3d* b, long long step, float* probe_row, cudaStream_t st) {
+// One leapfrog step of every grid (kernels only; capturable).  TMA batches
+// read buffer set `in_set` and write the other one.
+int batch_launch_step(jxf_batch3d* b, long long step, float* probe_row, cudaStream_t st,
+                      int in_set = 0) {
+  if (b->tma) {
+    TRY(batch_tma_launch(b, in_set, st));
+    if (b->band.band) TRY(band_launch(b->band, st, in_set ^ 1));
+    if (probe_row && b->n_probes > 0)
+      k3d_batch_probes<<<(b->n_probes + 127) / 128, 128, 0, st>>>(
+          b->d_tparams + (size_t)(in_set ^ 1) * b->grids.size(), b->d_probes, b->n_probes,
+          probe_row);
+    CUDA_TRY(cudaGetLastError());
+    return JXF_OK;
+  }
   BatchBlocks bb{b->d_params, b->d_blk_grid, b->d_blk_first, b->d_blk_count};
   if (b->mode == MODE_CPML) {
     k3d_batch_h<MODE_CPML><<<b->n_blocks, 256, 0, st>>>(bb);
@@ -2325,25 +2521,117 @@ int batch_launch_step(jxf_batch3d* b, long long step, float* probe_row, cudaStre
 
 }  // namespace
 
+namespace {
+
+// Launch shape of a TMA batch: every registry shape offered for batches x
+// chunk {4, 8, 16} x single-axis split (CPML, kappa = 1), each timed over two
+// steps into the idle buffer sets (the state is untouched), best of two
+// trials.  JXF_BATCH_LAUNCH=cfg,chunk[,split] pins it.
+int batch_tma_tune(jxf_batch3d* b, int in_set, cudaStream_t st) {
+  b->tuned = true;
+  const char* forced = std::getenv("JXF_BATCH_LAUNCH");
+  int fc = -1, fk = -1, fs = 0;
+  if (forced && std::sscanf(forced, "%d,%d,%d", &fc, &fk, &fs) >= 2 && fc >= 0 &&
+      fc < (int)tma_configs().size() && tma_configs()[fc].kb[0][0] && fk >= 1) {
+    b->cfg = fc;
+    b->chunk = fk;
+    b->axis_split = fs != 0 ? 1 : 0;
+    return JXF_OK;
+  }
+  const char* env = std::getenv("JXF_AUTOTUNE");
+  if (env && env[0] == '0') return JXF_OK;
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int bc = b->cfg, bk = b->chunk, bs = b->axis_split;
+  const bool can_split = b->mode == MODE_CPML && !b->kappa;
+  for (int sp = 0; sp < (can_split ? 2 : 1); ++sp)
+    for (int ci = 0; ci < (int)tma_configs().size(); ++ci) {
+      if (!tma_configs()[ci].kb[0][0]) continue;
+      for (int ch : {4, 8, 16}) {
+        b->cfg = ci;
+        b->chunk = ch;
+        b->axis_split = sp;
+        bool moved = false;
+        TRY(batch_tma_tables(b, &moved));
+        TRY(batch_tma_launch(b, in_set, st));
+        float ms = 1e30f;
+        for (int trial = 0; trial < 2; ++trial) {
+          CUDA_TRY(cudaEventRecord(e0, st));
+          for (int r = 0; r < 2; ++r) TRY(batch_tma_launch(b, in_set, st));
+          CUDA_TRY(cudaEventRecord(e1, st));
+          CUDA_TRY(cudaEventSynchronize(e1));
+          float t = 0;
+          CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+          ms = std::min(ms, t);
+        }
+        if (ms < best) {
+          best = ms;
+          bc = ci;
+          bk = ch;
+          bs = sp;
+        }
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->cfg = bc;
+  b->chunk = bk;
+  b->axis_split = bs;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return JXF_OK;
+}
+
+}  // namespace
+
 extern "C" int jxf_batch3d_create(int32_t n, jxf_grid3d* const* grids, jxf_batch3d** out) {
   if (!out || n < 1 || !grids) return fail(JXF_ERR_INVALID, "need at least one grid");
   *out = nullptr;
+  if (!grids[0]) return fail(JXF_ERR_INVALID, "grid 0 is null");
   const int mode = grids[0]->mode;
   const int dev = grids[0]->d.device;
+  const int path = grids[0]->path;
   for (int i = 0; i < n; ++i) {
     const jxf_grid3d* g = grids[i];
     if (!g) return fail(JXF_ERR_INVALID, "grid %d is null", i);
-    if (g->path != JXF_PATH_GENERIC || g->slab)
-      return fail(JXF_ERR_INVALID, "grid %d: batched grids use the generic path", i);
+    if (g->slab) return fail(JXF_ERR_INVALID, "grid %d: x-slab grids are not batched", i);
+    if (g->path != path)
+      return fail(JXF_ERR_INVALID, "grid %d: batched grids share the kernel path", i);
     if (g->mode != mode || g->d.device != dev)
       return fail(JXF_ERR_INVALID, "grid %d: batched grids share the boundary mode and device", i);
     if (g->mode == MODE_PERIODIC) return fail(JXF_ERR_INVALID, "periodic grids are not batched");
+    if (path == JXF_PATH_TMA) {
+      if ((g->cb != nullptr) != (grids[0]->cb != nullptr))
+        return fail(JXF_ERR_INVALID,
+                    "grid %d: TMA batches need a permittivity map on every grid or on none", i);
+      if (g->kappa != grids[0]->kappa)
+        return fail(JXF_ERR_INVALID, "grid %d: TMA batches share the CPML kappa grading", i);
+      if (g->band.band)
+        return fail(JXF_ERR_INVALID, "grid %d: attach the band to the batch, not the grid", i);
+    }
   }
   DeviceGuard dg(dev);
   jxf_batch3d* b = new jxf_batch3d();
   b->grids.assign(grids, grids + n);
   b->mode = mode;
   b->device = dev;
+  b->tma = path == JXF_PATH_TMA;
+  b->cbarr = grids[0]->cb != nullptr;
+  b->kappa = grids[0]->kappa;
+  {
+    const char* e = std::getenv("JXF_PDL");
+    b->use_pdl = !(e && e[0] == '0');
+  }
+  if (b->tma) {
+    // a first launch shape; jxf_batch3d_step tunes it on the first run
+    b->cfg = 0;
+    b->chunk = 8;
+    b->axis_split = 0;
+  }
   int rc = batch_refresh(b);
   if (rc != JXF_OK) {
     jxf_batch3d_destroy(b);
@@ -2368,6 +2656,10 @@ extern "C" int jxf_batch3d_destroy(jxf_batch3d* b) {
   dfree(b->d_src_entries);
   dfree(b->d_probes);
   dfree(b->d_probe_buf);
+  dfree(b->d_tparams);
+  dfree(b->d_tmaps);
+  dfree(b->d_items);
+  dfree(b->d_counters);
   band_release(b->band);
   delete b;
   return JXF_OK;
@@ -2389,6 +2681,16 @@ extern "C" int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_gra
       return fail(JXF_ERR_INVALID, "a member grid's waveform table is too short");
   }
   DeviceGuard dg(b->device);
+  int in_set = 0;
+  if (b->tma) {
+    in_set = b->grids[0]->cur;
+    for (jxf_grid3d* g : b->grids)
+      if (g->cur != in_set)
+        return fail(JXF_ERR_INVALID,
+                    "TMA batch members must hold their state in the same buffer set (step "
+                    "parity); reset the batch or step the grids to equal parity");
+    if (!b->tuned) TRY(batch_tma_tune(b, in_set, (cudaStream_t)stream));
+  }
   TRY(batch_refresh(b));
   const size_t need = (size_t)n_steps * std::max(b->n_probes, 1);
   if (need > b->probe_cap) {
@@ -2404,14 +2706,16 @@ extern "C" int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_gra
   if (!use_graph) {
     for (int k = 0; k < n_steps; ++k)
       TRY(batch_launch_step(b, b->step + k,
-                            b->n_probes ? b->d_probe_buf + (size_t)k * b->n_probes : nullptr, st));
+                            b->n_probes ? b->d_probe_buf + (size_t)k * b->n_probes : nullptr, st,
+                            in_set ^ (k & 1)));
   } else {
     if (!b->own) {
       CUDA_TRY(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
       CUDA_TRY(cudaEventCreateWithFlags(&b->ev0, cudaEventDisableTiming));
       CUDA_TRY(cudaEventCreateWithFlags(&b->ev1, cudaEventDisableTiming));
     }
-    if (!b->graph || b->graph_n != n_steps || b->graph_step0 != b->step) {
+    if (!b->graph || b->graph_n != n_steps || b->graph_step0 != b->step ||
+        b->graph_set != in_set) {
       if (b->graph) cudaGraphExecDestroy(b->graph);
       b->graph = nullptr;
       cudaGraph_t graph;
@@ -2419,7 +2723,7 @@ extern "C" int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_gra
       for (int k = 0; k < n_steps; ++k) {
         int rc = batch_launch_step(
             b, b->step + k, b->n_probes ? b->d_probe_buf + (size_t)k * b->n_probes : nullptr,
-            b->own);
+            b->own, in_set ^ (k & 1));
         if (rc != JXF_OK) {
           cudaStreamEndCapture(b->own, &graph);
           return rc;
@@ -2430,6 +2734,7 @@ extern "C" int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_gra
       cudaGraphDestroy(graph);
       b->graph_n = n_steps;
       b->graph_step0 = b->step;
+      b->graph_set = in_set;
     }
     // order the graph between the caller's earlier and later work
     CUDA_TRY(cudaEventRecord(b->ev0, st));
@@ -2439,7 +2744,31 @@ extern "C" int jxf_batch3d_step(jxf_batch3d* b, int32_t n_steps, int32_t use_gra
     CUDA_TRY(cudaStreamWaitEvent(st, b->ev1, 0));
   }
   b->step += n_steps;
-  for (jxf_grid3d* g : b->grids) g->step += n_steps;
+  for (jxf_grid3d* g : b->grids) {
+    g->step += n_steps;
+    if (b->tma) g->cur ^= (n_steps & 1);
+  }
+  return JXF_OK;
+}
+
+extern "C" int jxf_batch3d_kernels_per_step(const jxf_batch3d* b) {
+  if (!b) return 0;
+  int n = 0;
+  if (b->tma) {
+    for (int i = 0; i < 5; ++i) n += b->part_n[i] > 0 ? 1 : 0;
+  } else {
+    n = 2 + (b->n_src_entries > 0 ? 1 : 0);
+  }
+  if (b->band.band) n += 2;
+  if (b->n_probes > 0) n += 1;
+  return n;
+}
+
+extern "C" int jxf_batch3d_launch(const jxf_batch3d* b, int32_t* out3) {
+  if (!b || !out3) return fail(JXF_ERR_INVALID, "null argument");
+  out3[0] = b->tma ? b->cfg : -1;
+  out3[1] = b->tma ? b->chunk : -1;
+  out3[2] = b->tma ? b->axis_split : -1;
   return JXF_OK;
 }
 
@@ -2562,10 +2891,12 @@ int band_check_dims(int nx, int ny, int nz) {
   return JXF_OK;
 }
 
-int band_launch(const BandTables& t, cudaStream_t st) {
+// Band correction of the state held in buffer set `set` of every grid.
+int band_launch(const BandTables& t, cudaStream_t st, int set) {
   if (t.tiles <= 0) return JXF_OK;
+  const band::GridRef* grids = (set != 0 && t.d_grids_b) ? t.d_grids_b : t.d_grids;
   band::InferArgs a{};
-  a.grids = t.d_grids;
+  a.grids = grids;
   a.cells = t.d_cells;
   a.tile_face = t.d_tile_face;
   a.n_tiles = t.tiles;
@@ -2576,7 +2907,7 @@ int band_launch(const BandTables& t, cudaStream_t st) {
   a.wait_ns = wait_limit_ns();
   band::k_band_infer<band::SRC_GRIDS><<<t.ctas, 128, band::kInfSmem, st>>>(a);
   const int n = t.tiles * band::kTile;
-  band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(t.d_grids, t.d_cells, n, t.d_delta);
+  band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(grids, t.d_cells, n, t.d_delta);
   CUDA_TRY(cudaGetLastError());
   return JXF_OK;
 }
@@ -2584,6 +2915,7 @@ int band_launch(const BandTables& t, cudaStream_t st) {
 void band_release(BandTables& t) {
   if (t.band) t.band->attached -= 1;
   dfree(t.d_grids);
+  dfree(t.d_grids_b);
   dfree(t.d_cells);
   dfree(t.d_tile_face);
   dfree(t.d_delta);
@@ -2695,7 +3027,7 @@ int band_train_pass(jxf_band* m, const band::TrainArgs& a, cudaStream_t st) {
 int band_attach(const std::vector<jxf_grid3d*>& grids, jxf_band* m, int device, int64_t* tally,
                 BandTables& t) {
   if (m->device != device) return fail(JXF_ERR_INVALID, "band and grids on different devices");
-  std::vector<band::GridRef> refs;
+  std::vector<band::GridRef> refs, refs_b;
   std::vector<int2> per[6];
   std::vector<int> cells[6];
   for (size_t k = 0; k < grids.size(); ++k) {
@@ -2709,6 +3041,8 @@ int band_attach(const std::vector<jxf_grid3d*>& grids, jxf_band* m, int device, 
     r.ny = g->d.ny;
     r.nz = g->d.nz;
     refs.push_back(r);
+    for (int c = 0; c < 6; ++c) r.f[c] = g->f[1][c];
+    refs_b.push_back(r);
     band_cells(g->d.nx, g->d.ny, g->d.nz, cells);
     for (int f = 0; f < 6; ++f)
       for (int c : cells[f]) per[f].push_back(make_int2(c, (int)k));
@@ -2718,6 +3052,7 @@ int band_attach(const std::vector<jxf_grid3d*>& grids, jxf_band* m, int device, 
   band_tiles(per, tc, tf);
   BandTables n{};
   int rc = upload(&n.d_grids, refs, tally);
+  if (rc == JXF_OK) rc = upload(&n.d_grids_b, refs_b, tally);
   if (rc == JXF_OK) rc = upload(&n.d_cells, tc, tally);
   if (rc == JXF_OK) rc = upload(&n.d_tile_face, tf, tally);
   if (rc == JXF_OK) rc = dmalloc(&n.d_delta, tc.size() * band::kOut, tally);

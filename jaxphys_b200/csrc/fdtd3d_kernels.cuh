@@ -563,9 +563,12 @@ __device__ __forceinline__ void slab_first_cell(int t, int z0, int y0, int nz, i
 // AXES (CPML only): the slab axes the block's cells may touch (1 = x, 2 = y,
 // 4 = z); the code and psi storage of the other axes compile away.  The host
 // launches single-axis variants for blocks that touch one slab axis only.
+// One block of work: the tile (tzi, tyi) over x chunk ci.  Called by the
+// single-grid kernel (one block per work item) and by the batch kernel (a
+// persistent block looping over the items of many grids).
 template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA, int AXES = 7>
-__global__ void __launch_bounds__(TZ*(TY / RY))
-    k3d_tma(const __grid_constant__ Step3D p, const __grid_constant__ Maps3D maps) {
+__device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, int tzi, int tyi,
+                                          int ci, bool slab_first) {
   constexpr bool CPML = (MODE == MODE_CPML);
   constexpr bool AX = (AXES & 1) != 0, AY = (AXES & 2) != 0, AZ = (AXES & 4) != 0;
   using L = TmaLayout<TZ, TY, RY, STAGES, CBARR, CPML, AXES>;
@@ -590,15 +593,6 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
 
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int tid = threadIdx.x;
-  int tzi = blockIdx.x, tyi = blockIdx.y, ci = blockIdx.z;
-  bool slab_first = false;
-  if (p.blk_list != nullptr) {
-    tzi = p.blk_list[3 * blockIdx.x];
-    tyi = p.blk_list[3 * blockIdx.x + 1];
-    const int v = p.blk_list[3 * blockIdx.x + 2];
-    ci = v & BLK_CHUNK_MASK;
-    slab_first = (v & BLK_SLAB_FIRST) != 0;
-  }
   const int z0 = tzi * TZ;
   const int y0 = tyi * TY;
   int tx = tid % TZ;
@@ -612,14 +606,6 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   const int nload = qe - qs + 1;
   const float a = p.a;
   const int z = z0 + tx;
-
-  // Programmatic dependent launch: a step kernel waits for the previous
-  // step's grids before touching its inputs and then lets the next launch be
-  // scheduled; the plain interior kernel of a CPML step overlaps the shell
-  // kernel it depends on and only waits for it before exiting (so the next
-  // step, which waits on the interior kernel, also sees the shell's writes).
-  if (p.pdl & PDL_WAIT_START) grid_dep_wait();
-  if (p.pdl & PDL_TRIGGER) grid_dep_launch_dependents();
 
   // Probes of the input state (= after the previous step).
   if (p.probe_out != nullptr && tzi == 0 && tyi == 0 && ci == 0) {
@@ -1107,7 +1093,96 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
     }
     __syncthreads();
   }
+}
+
+template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA, int AXES = 7>
+__global__ void __launch_bounds__(TZ*(TY / RY))
+    k3d_tma(const __grid_constant__ Step3D p, const __grid_constant__ Maps3D maps) {
+  int tzi = blockIdx.x, tyi = blockIdx.y, ci = blockIdx.z;
+  bool slab_first = false;
+  if (p.blk_list != nullptr) {
+    tzi = p.blk_list[3 * blockIdx.x];
+    tyi = p.blk_list[3 * blockIdx.x + 1];
+    const int v = p.blk_list[3 * blockIdx.x + 2];
+    ci = v & BLK_CHUNK_MASK;
+    slab_first = (v & BLK_SLAB_FIRST) != 0;
+  }
+  // Programmatic dependent launch: a step kernel waits for the previous
+  // step's grids before touching its inputs and then lets the next launch be
+  // scheduled; the plain interior kernel of a CPML step overlaps the shell
+  // kernel it depends on and only waits for it before exiting (so the next
+  // step, which waits on the interior kernel, also sees the shell's writes).
+  if (p.pdl & PDL_WAIT_START) grid_dep_wait();
+  if (p.pdl & PDL_TRIGGER) grid_dep_launch_dependents();
+  tma_block<TZ, TY, RY, STAGES, MODE, CBARR, KAPPA, AXES>(p, maps, tzi, tyi, ci, slab_first);
   if (p.pdl & PDL_WAIT_END) grid_dep_wait();
+}
+
+// Batches of grids on the TMA kernel: one persistent launch per step (and per
+// CPML part) over a work list of (grid, tile, chunk) items of every grid,
+// heaviest first.  Blocks take items through an atomic counter; the last
+// block to finish resets the counter for the next launch (which reads it only
+// after its programmatic-dependent-launch wait, i.e. after this grid is done).
+struct TmaBatchArgs {
+  const Step3D* params;  // [2][n_grids]: parameters with input set 0 / 1
+  const Maps3D* maps;    // [2][n_grids]
+  int n_grids;
+  int in_set;            // input set of this step (one parity for the batch)
+  const int4* items;     // (grid, tile_z, tile_y, chunk word)
+  int n_items;
+  int* counter;          // [0] next item, [1] blocks done
+  int pdl;
+};
+
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// the tensor maps live in global memory (written by the host before launch)
+__device__ __forceinline__ void tensormap_acquire(const void* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                   reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
+template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA, int AXES = 7>
+__global__ void __launch_bounds__(TZ*(TY / RY))
+    k3d_tma_batch(const __grid_constant__ TmaBatchArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  __shared__ int s_item;
+  if (a.pdl & PDL_WAIT_START) grid_dep_wait();
+  if (a.pdl & PDL_TRIGGER) grid_dep_launch_dependents();
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&a.counter[0], 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= a.n_items) break;
+    const int4 w = a.items[it];
+    const int k = a.in_set * a.n_grids + w.x;
+    const Maps3D& m = a.maps[k];
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < 3; ++c) {
+        tensormap_acquire(&m.e[c]);
+        tensormap_acquire(&m.h[c]);
+      }
+      if (CBARR) tensormap_acquire(&m.cb);
+    }
+    tma_block<TZ, TY, RY, STAGES, MODE, CBARR, KAPPA, AXES>(
+        a.params[k], m, w.y, w.z, w.w & BLK_CHUNK_MASK, (w.w & BLK_SLAB_FIRST) != 0);
+    __syncthreads();  // every wait of the item is over
+    if (threadIdx.x == 0)
+      for (int s = 0; s < STAGES; ++s) mbar_inval(&bars[s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.counter[1], 1) == (int)gridDim.x - 1) {
+      a.counter[0] = 0;
+      a.counter[1] = 0;
+      __threadfence();
+    }
+  }
+  if (a.pdl & PDL_WAIT_END) grid_dep_wait();
 }
 
 }  // namespace jxf

@@ -1,12 +1,22 @@
 """Batches of independent 3D grids advanced together (extension).
 
-``FDTDBatch(grids)`` takes ``EMGrid3D`` objects (generic kernel path; any
-mix of sizes, including odd ones; one boundary mode) and advances all of them
-with one kernel per phase per step over the whole batch (C ABI
-``jxf_batch3d_*``).  ``run(n)`` captures the n-step sequence once into a CUDA
-graph and replays it with a single launch.  Each grid keeps its own
-permittivity, sources, probes and field accessors.  Typical use: many design
-candidates, or many source positions, of one device.
+``FDTDBatch(grids)`` takes ``EMGrid3D`` objects of any mix of sizes and one
+boundary mode, all on one kernel path, and advances all of them together (C
+ABI ``jxf_batch3d_*``):
+
+* TMA path (nz % 4 == 0; ``path="auto"`` or ``"tma"``): one persistent launch
+  per step (and per CPML part) over a work list of every grid's
+  (tile, x-chunk) blocks, heaviest first; blocks take work through an atomic
+  counter.  The launch shape (tile, chunk, single-axis CPML split) is tuned
+  per batch on the first run.  Every grid must hold its state in the same
+  buffer set (same step parity), and all or none carry a permittivity map.
+* generic path: one kernel per phase per step over the whole batch (any
+  shape, odd nz included).
+
+``run(n)`` captures the n-step sequence once into a CUDA graph and replays it
+with a single launch.  Each grid keeps its own permittivity, sources, probes
+and field accessors.  Typical use: many design candidates, or many source
+positions, of one device.
 """
 
 from __future__ import annotations
@@ -21,13 +31,17 @@ class FDTDBatch:
     def __init__(self, grids):
         if not grids:
             raise ConfigurationError("empty batch")
+        paths = set()
         for g in grids:
-            if g._path != "generic":
-                raise ConfigurationError("batched grids must be built with path='generic'")
             if g._h is None:
                 g.prepare(g._dt, g._t_start)
             elif g._dirty:
                 g._upload_config()
+            paths.add(g.info()["path"])
+        if len(paths) != 1:
+            raise ConfigurationError("batched grids must all use one kernel path (build them "
+                                     "with the same path=)")
+        self.path = "tma" if paths == {nat.PATH_TMA} else "generic"
         self.grids = list(grids)
         lib = nat.load()
         arr = (C.c_void_p * len(grids))(*[g._h for g in grids])
@@ -49,6 +63,17 @@ class FDTDBatch:
         nat.check(nat.load().jxf_batch3d_set_band(self._h, None if model is None else model._h),
                   "jxf_batch3d_set_band")
         self.band = model
+
+    def kernels_per_step(self) -> int:
+        """Kernel launches per leapfrog step of the last run's shape."""
+        return int(nat.load().jxf_batch3d_kernels_per_step(self._h))
+
+    def launch(self) -> dict:
+        """Launch shape of a TMA batch: registry entry, x chunk, single-axis
+        split (all -1 on the generic path)."""
+        v = (C.c_int32 * 3)()
+        nat.check(nat.load().jxf_batch3d_launch(self._h, v), "jxf_batch3d_launch")
+        return {"tma_config": v[0], "x_chunk": v[1], "axis_split": v[2]}
 
     def close(self):
         if self._h is not None:

@@ -316,10 +316,14 @@ def test_config3_512_cpml12_smooth_eps(cuda):
     """Config 3: 512^3 FP32, 200 steps, 12-cell CPML (m=3, R0=1e-6), eps_r
     from seeded uniform noise smoothed by a Gaussian (sigma = 6 cells) and
     rescaled to [1, 12], Gaussian-modulated Ez dipole at the centre (f0 =
-    0.05/dt, width 30 steps), 16 seeded interior Ez probes.  Checked against
-    the FP64 C oracle: probe traces over the whole run and the E and H fields
-    after step 200 (the pulse is still inside the box), relative L2 <= 1e-5
-    (tolerance of the 3D FP32 path)."""
+    0.05/dt, width 30 steps), 16 seeded Ez probes.  Checked against the FP64
+    C oracle: probe traces over the whole run and the E and H fields after
+    step 200 (the pulse is still inside the box), relative L2 <= 1e-5
+    (tolerance of the 3D FP32 path).  The probes sit within 20 cells of the
+    source: in 200 steps the pulse (peak at step 120, eps_r ~ 6.5 on average)
+    travels ~30 cells, and probes further out would see only the Yee
+    stencil's precursor (FP64 values of 1e-40 and below), which FP32 cannot
+    represent and which says nothing about the kernel."""
     import psutil
     from scipy.ndimage import gaussian_filter
 
@@ -335,7 +339,9 @@ def test_config3_512_cpml12_smooth_eps(cuda):
     u = (u - u.min()) / (u.max() - u.min())
     eps = (1.0 + 11.0 * u.astype(np.float64))
     del u
-    probes = _cfg_probes(n, 16, seed=3)
+    prng = np.random.default_rng(3)
+    probes = [tuple(int(n // 2 + v) for v in prng.integers(-20, 21, size=3)) + (2,)
+              for _ in range(16)]
     src = [_gauss((n // 2, n // 2, n // 2), width=30.0)]
     g = _cpml_grid("auto", (n, n, n), None, src, probes, n_pml=pml)
     g.set_permittivity(eps)
@@ -350,6 +356,7 @@ def test_config3_512_cpml12_smooth_eps(cuda):
     del eps
     o = Oracle3DC(spec, dt=dt)
     out = o.run(steps)
+    assert np.abs(out["probes"]).max() > 1e-4  # the probes see the pulse
     assert rel_l2(tr, out["probes"]) <= TOL
     eE = _rel_l2_by_component(lambda c: to_np(g.field(COMPS[c])), o.f, (0, 1, 2))
     eH = _rel_l2_by_component(lambda c: to_np(g.field(COMPS[c])), o.f, (3, 4, 5))
