@@ -359,6 +359,18 @@ def run_ours(args, world, rank, local, pg, workload=None, steps=None, warmup=Non
     return line
 
 
+def pack_by_cells(cells: list, parts: int) -> list:
+    """Indices of each part: largest item first onto the least-loaded part."""
+    order = sorted(range(len(cells)), key=lambda i: -cells[i])
+    load = [0] * parts
+    out = [[] for _ in range(parts)]
+    for i in order:
+        r = min(range(parts), key=lambda k: load[k])
+        out[r].append(i)
+        load[r] += cells[i]
+    return [sorted(o) for o in out]
+
+
 def c5_cases(seed: int = 5, n_grids: int = 64):
     """The batched learned-boundary workload: seeded interior sides uniform in
     [48, 160] (half cubes, half boxes), smoothed eps_r in [1, 6], one dipole of
@@ -394,8 +406,13 @@ def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=
 
     torch.cuda.set_device(local)
     n_grids, nsteps, _, wname = WORKLOADS["c5"]
-    cases = c5_cases(seed=5 + rank, n_grids=n_grids)
+    # the 64 grids are bin-packed by cell count over the ranks (largest first
+    # onto the least-loaded rank): a fixed total batch, so strong scaling
+    all_cases = c5_cases(seed=5, n_grids=n_grids)
+    cases = [all_cases[i] for i in pack_by_cells([int(np.prod(c.size)) for c in all_cases],
+                                                 world)[rank]]
     interior = sum(int(np.prod(c.size)) for c in cases)
+    interior_total = sum(int(np.prod(c.size)) for c in all_cases)
     model = LearnedBand.load(BAND_WEIGHTS) if BAND_WEIGHTS.exists() else train_band(seed=0)
     stream = torch.cuda.current_stream()
 
@@ -427,6 +444,11 @@ def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=
     for kind in ("learned", "cpml10", "cpml4", "pec"):
         grids, b = build(kind)
         cells = sum(int(np.prod(g.size)) for g in grids)
+        cells_total = cells
+        if pg is not None:
+            t = torch.tensor([float(cells)], dtype=torch.float64, device=f"cuda:{local}")
+            pg.all_reduce(t)
+            cells_total = int(t.item())
         for _ in range(max(n_warm, 1)):
             b.reset()
             b.run(nsteps)
@@ -450,9 +472,9 @@ def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=
             ms = float(t.item())
         for g in grids[:2]:
             g.check()
-        results[kind] = {"ms_per_step": round(ms / n_timed, 3), "grid_cells": cells,
-                         "interior_gcell_s": round(interior * nsteps * n_timed * world / ms / 1e6, 3),
-                         "grid_gcell_s": round(cells * nsteps * n_timed * world / ms / 1e6, 3)}
+        results[kind] = {"ms_per_step": round(ms / n_timed, 3), "grid_cells": cells_total,
+                         "interior_gcell_s": round(interior_total * nsteps * n_timed / ms / 1e6, 3),
+                         "grid_gcell_s": round(cells_total * nsteps * n_timed / ms / 1e6, 3)}
         if kind == "learned":
             results[kind]["clocks"] = clocks
             launches = b.kernels_per_step() * nsteps * n_timed
@@ -474,9 +496,10 @@ def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=
     # band (outer cells: 24 B stencil centre read, 24 B correction written
     # and read back, 24 B field read-modify-write: 120 B per outer cell)
     outer = sum(int(np.prod(np.array(c.size) + 6)) - int(np.prod(np.array(c.size) + 4))
-                for c in cases)
+                for c in all_cases)
     step_bytes = lr["grid_cells"] * 52.0 + outer * 120.0
-    achieved = step_bytes / (lr["ms_per_step"] / nsteps * 1e-3) / 1e9
+    # per GPU (the batch is split over the ranks)
+    achieved = step_bytes / world / (lr["ms_per_step"] / nsteps * 1e-3) / 1e9
     line = {
         "metric": "learned-band batch interior Gcell-updates/s",
         "value": lr["interior_gcell_s"],
@@ -486,15 +509,15 @@ def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=
         "warmup": n_warm,
         "ms_per_step": lr["ms_per_step"],
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32 fields, bf16 MLP with f32 accumulation",
         "data": "synthetic (seeded sizes, eps_r maps, dipoles)",
-        "config": {"workload": wname, "grids": n_grids, "interior_cells": interior,
+        "config": {"workload": wname, "grids": n_grids, "interior_cells": interior_total,
                    "leapfrog_steps_per_step": nsteps, "band_layers": BAND_LAYERS,
                    "l2": "inputs larger than L2 (>= 360 MB of fields)",
                    "path": "tma (persistent batch launch)", "launch": lr.pop("launch", None),
-                   "parallelism": f"independent batch per GPU x{world}"},
+                   "parallelism": f"the 64 grids bin-packed by cell count over {world} GPU(s)"},
         "compare": {k: results[k] for k in ("cpml10", "cpml4", "pec")},
         "speedup_vs_cpml10": round(results["cpml10"]["ms_per_step"] / lr["ms_per_step"], 3),
         "speedup_vs_cpml4_equal_error": round(results["cpml4"]["ms_per_step"] / lr["ms_per_step"], 3),

@@ -185,6 +185,15 @@ int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_grad, float* g
 int jxf_grid3d_create_slab(const jxf_grid3d_desc* desc, int32_t x0, int32_t x1,
                            jxf_grid3d** out);
 int jxf_grid3d_half_step(jxf_grid3d* g, int32_t half, float* probe_row, void* stream);
+/* The same half-step in two parts, so the exchange with a neighbour overlaps
+ * the bulk of the update: part 1 updates only the plane this half-step hands
+ * to a neighbour (H: the last owned plane; E: the first owned plane, with its
+ * sources), part 2 the other owned planes (E: with their sources, then the
+ * probes; the step counter advances after E part 2).  part 0 = the whole
+ * half-step.  Same results as jxf_grid3d_half_step bit for bit.  No reference
+ * counterpart (the reference runs on one device). */
+int jxf_grid3d_half_step_part(jxf_grid3d* g, int32_t half, int32_t part, float* probe_row,
+                              void* stream);
 int jxf_grid3d_plane(jxf_grid3d* g, int32_t comp, int32_t plane, float* buf, int32_t to_buf,
                      void* stream);
 

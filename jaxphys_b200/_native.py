@@ -122,6 +122,7 @@ SIGNATURES = {
     "jxf_grid3d_adjoint_backward": (C.c_int, [_vp, _vp, _vp, _vp]),
     "jxf_grid3d_create_slab": (C.c_int, [C.POINTER(Grid3DDesc), _i32, _i32, C.POINTER(_vp)]),
     "jxf_grid3d_half_step": (C.c_int, [_vp, _i32, _vp, _vp]),
+    "jxf_grid3d_half_step_part": (C.c_int, [_vp, _i32, _i32, _vp, _vp]),
     "jxf_grid3d_plane": (C.c_int, [_vp, _i32, _i32, _vp, _i32, _vp]),
     "jxf_batch3d_create": (C.c_int, [_i32, C.POINTER(_vp), C.POINTER(_vp)]),
     "jxf_batch3d_destroy": (C.c_int, [_vp]),

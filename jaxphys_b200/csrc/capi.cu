@@ -1732,6 +1732,93 @@ int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stre
   return JXF_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Soft sources of the cells whose plane lies in [plo, phi) (slab half-steps
+// split into a boundary plane and the rest).
+__global__ void k3d_sources_planes(float* ex, float* ey, float* ez, const SrcCell* cells,
+                                   int n_cells, const SrcTerm* terms, const float* wave,
+                                   long long wave_len, long long step, long long plane, int plo,
+                                   int phi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_cells) return;
+  const SrcCell c = cells[i];
+  const long long x = c.cell / plane;
+  if (x < plo || x >= phi) return;
+  float* f = c.comp == 0 ? ex : (c.comp == 1 ? ey : ez);
+  float v = f[c.cell];
+  for (int k = 0; k < c.count; ++k) {
+    const SrcTerm t = terms[c.first + k];
+    v = fadd(v, fmul(t.amp, wave[(long long)t.wave * wave_len + step]));
+  }
+  f[c.cell] = v;
+}
+}  // namespace
+
+extern "C" {
+
+int jxf_grid3d_half_step_part(jxf_grid3d* g, int32_t half, int32_t part, float* probe_row,
+                              void* stream) {
+  if (!g) return fail(JXF_ERR_INVALID, "null handle");
+  if (!g->slab) return fail(JXF_ERR_INVALID, "half steps are for x-slab grids");
+  if (half != 0 && half != 1) return fail(JXF_ERR_INVALID, "half must be 0 (H) or 1 (E)");
+  if (part < 0 || part > 2) return fail(JXF_ERR_INVALID, "part must be 0, 1 or 2");
+  if (part == 0) return jxf_grid3d_half_step(g, half, probe_row, stream);
+  if (g->x_hi - g->x_lo < 2)
+    return fail(JXF_ERR_INVALID, "a split half-step needs at least two owned planes");
+  if (half == 1 && !g->src_cell.empty()) {
+    int max_w = 0;
+    for (int w : g->src_wave) max_w = std::max(max_w, w);
+    if (max_w >= g->n_waves || g->step + 1 > g->wave_len)
+      return fail(JXF_ERR_INVALID, "waveform table does not cover step %lld", g->step);
+  }
+  DeviceGuard dg(g->d.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  Step3D p = base_params(g);
+  set_io(g, p, 0, 0);
+  p.step = g->step;
+  // the plane this half-step hands to a neighbour: H of the last owned plane
+  // (the next rank's E needs it), E of the first owned plane (the previous
+  // rank's H needs it); part 2 is the rest of the owned planes
+  const int bplane = half == 0 ? g->x_hi - 1 : g->x_lo;
+  if (part == 1) {
+    p.x_lo = bplane;
+    p.x_hi = bplane + 1;
+  } else if (half == 0) {
+    p.x_hi = g->x_hi - 1;
+  } else {
+    p.x_lo = g->x_lo + 1;
+  }
+  const int threads = 256;
+  const long long owned = (long long)(p.x_hi - p.x_lo) * g->d.ny * g->d.nz;
+  const int blocks = (int)std::min<long long>((owned + threads - 1) / threads, 148LL * 16);
+  if (half == 0) {
+    if (g->mode == MODE_CPML)
+      jxf::k3d_generic_h<MODE_CPML><<<blocks, threads, 0, st>>>(p);
+    else
+      jxf::k3d_generic_h<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+    CUDA_TRY(cudaGetLastError());
+    return JXF_OK;
+  }
+  if (g->mode == MODE_CPML)
+    jxf::k3d_generic_e<MODE_CPML><<<blocks, threads, 0, st>>>(p);
+  else
+    jxf::k3d_generic_e<MODE_ABSORB><<<blocks, threads, 0, st>>>(p);
+  CUDA_TRY(cudaGetLastError());
+  if (g->n_cells > 0) {
+    k3d_sources_planes<<<(g->n_cells + 127) / 128, 128, 0, st>>>(
+        g->f[0][0], g->f[0][1], g->f[0][2], g->d_cells, g->n_cells, g->d_terms, g->d_wave,
+        g->wave_len, g->step, (long long)g->d.ny * g->d.nz, p.x_lo, p.x_hi);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (part == 2) {  // the E half-step ends with its second part
+    if (probe_row && g->n_probes > 0) TRY(gather_probes(g, 0, probe_row, st));
+    g->step++;
+  }
+  return JXF_OK;
+}
+
 int jxf_grid3d_half_step(jxf_grid3d* g, int32_t half, float* probe_row, void* stream) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
   if (!g->slab) return fail(JXF_ERR_INVALID, "half steps are for x-slab grids");

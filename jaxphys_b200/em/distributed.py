@@ -16,7 +16,11 @@ neighbouring ranks, both of two tangential components of one plane:
 
 CPML psi state and the material stay local.  Point-to-point transfers go
 through the group's backend (NCCL over NVLink between GPUs; gloo through host
-memory).  Probe traces are all-reduced so every rank returns the full trace.
+memory).  With ``overlap=True`` (default) each half-step first updates the
+plane a neighbour needs, posts the swap, updates the remaining planes while
+the planes cross the link, and waits for the swap only before the half-step
+that reads the ghost plane.  Probe traces are all-reduced so every rank
+returns the full trace.
 """
 
 from __future__ import annotations
@@ -110,6 +114,11 @@ class CudaSlabStepper:
             self.h, half, None if probe_row is None else probe_row.data_ptr(),
             nat.stream_handle()), "jxf_grid3d_half_step")
 
+    def half_step_part(self, half: int, part: int, probe_row=None):
+        nat.check(self.lib.jxf_grid3d_half_step_part(
+            self.h, half, part, None if probe_row is None else probe_row.data_ptr(),
+            nat.stream_handle()), "jxf_grid3d_half_step_part")
+
     def new_probe_buffer(self, n_steps: int, n_local: int):
         return self.torch.zeros((n_steps, n_local), dtype=self.torch.float32, device=self.dev)
 
@@ -134,7 +143,7 @@ class DistributedGrid3D:
 
     def __init__(self, size, resolution=0.01, boundary="absorbing", pml_layers=8, *,
                  cpml: CPMLSpec | None = None, group=None, device: int | None = None,
-                 stepper_factory=None):
+                 stepper_factory=None, overlap: bool = True):
         import torch.distributed as dist
 
         self.dist = dist
@@ -171,6 +180,10 @@ class DistributedGrid3D:
         self.local_shape = (self.nloc + 2, self.size[1], self.size[2])
         self.step_count = 0
         self._configured = False
+        # overlap: each half-step updates the plane a neighbour needs first,
+        # exchanges it while the other planes update, and waits for the
+        # exchange only before the half-step that reads the ghost plane
+        self.overlap = bool(overlap) and self.nloc >= 2 and hasattr(self.st, "half_step_part")
 
     # ----------------------------------------------------------- set-up
     def add_source(self, s: PointSource3D):
@@ -227,6 +240,41 @@ class DistributedGrid3D:
         self._configured = True
 
     # ----------------------------------------------------------- exchange
+    def _start_exchange(self, comps, send_plane, direction):
+        """Post the swap of one plane of `comps` with the neighbours (send my
+        `send_plane` towards `direction`, receive the other neighbour's) and
+        return (works, receive buffer); the transfers run while the caller
+        queues more work on its stream."""
+        import torch
+
+        r = self.rank
+        if direction < 0:
+            send_to = r - 1 if r > 0 else None
+            recv_from = r + 1 if r < self.world - 1 else None
+        else:
+            send_to = r + 1 if r < self.world - 1 else None
+            recv_from = r - 1 if r > 0 else None
+        on_host = self.dist.get_backend(self.group) == "gloo"
+        dev = torch.device("cpu") if on_host else self.st.device
+        dtype = self.st.dtype
+        ops, recv = [], None
+        if recv_from is not None:
+            recv = torch.empty((len(comps), self.size[1], self.size[2]), dtype=dtype, device=dev)
+            ops.append(self.dist.P2POp(self.dist.irecv, recv, recv_from, self.group))
+        if send_to is not None:
+            send = torch.stack([self.st.get_plane(c, send_plane) for c in comps]).to(dev, dtype)
+            ops.append(self.dist.P2POp(self.dist.isend, send.contiguous(), send_to, self.group))
+        works = self.dist.batch_isend_irecv(ops) if ops else []
+        return works, recv
+
+    def _finish_exchange(self, pending, comps, recv_plane):
+        works, recv = pending
+        for w in works:
+            w.wait()
+        if recv is not None:
+            for k, c in enumerate(comps):
+                self.st.set_plane(c, recv_plane, recv[k])
+
     def _exchange(self, comps, send_plane, recv_plane, direction):
         """Swap one plane of `comps` with the neighbours: direction -1 sends
         my plane to rank-1 and receives rank+1's into recv_plane; +1 the
@@ -276,13 +324,31 @@ class DistributedGrid3D:
             self._wave_len = 2 * (self.step_count + n_steps)
             self.st.set_waveforms(wf.build_table(keys, self._wave_len, self.dt, 0.0))
         buf = self.st.new_probe_buffer(n_steps, len(self.own_probes))
-        for k in range(n_steps):
-            # Ey, Ez of the next rank's first plane -> my high ghost plane
+        if self.overlap:
+            # the E ghost plane of the current state
             self._exchange((1, 2), 1, self.nloc + 1, -1)
-            self.st.half_step(0)
-            # Hy, Hz of the previous rank's last plane -> my low ghost plane
-            self._exchange((4, 5), self.nloc, 0, +1)
-            self.st.half_step(1, buf[k] if len(self.own_probes) else None)
+        for k in range(n_steps):
+            row = buf[k] if len(self.own_probes) else None
+            if not self.overlap:
+                # Ey, Ez of the next rank's first plane -> my high ghost plane
+                self._exchange((1, 2), 1, self.nloc + 1, -1)
+                self.st.half_step(0)
+                # Hy, Hz of the previous rank's last plane -> my low ghost plane
+                self._exchange((4, 5), self.nloc, 0, +1)
+                self.st.half_step(1, row)
+                continue
+            # H: last owned plane (the next rank's E needs its Hy, Hz), post
+            # the swap, the other planes, then the low ghost plane
+            self.st.half_step_part(0, 1)
+            pend = self._start_exchange((4, 5), self.nloc, +1)
+            self.st.half_step_part(0, 2)
+            self._finish_exchange(pend, (4, 5), 0)
+            # E: first owned plane (the previous rank's H needs its Ey, Ez),
+            # post the swap, the other planes, then the high ghost plane
+            self.st.half_step_part(1, 1)
+            pend = self._start_exchange((1, 2), 1, -1)
+            self.st.half_step_part(1, 2, row)
+            self._finish_exchange(pend, (1, 2), self.nloc + 1)
         self.step_count += n_steps
         full = torch.zeros((n_steps, len(self.probes)), dtype=buf.dtype, device=buf.device)
         if self.own_probes:

@@ -65,10 +65,25 @@ class NumpySlabStepper:
     def field(self, comp, local_shape):
         return torch.from_numpy(self.f[comp].copy())
 
-    def half_step(self, half, probe_row=None):
+    def half_step_part(self, half, part, probe_row=None):
+        """Part 1: the plane handed to a neighbour (H: last owned plane, E:
+        first owned plane); part 2: the other owned planes (E: then probes and
+        the step counter)."""
+        if part == 0:
+            return self.half_step(half, probe_row)
+        b = self.nloc if half == 0 else 1
+        if part == 1:
+            lo, hi = b, b + 1
+        else:
+            lo, hi = (1, self.nloc) if half == 0 else (2, self.nloc + 1)
+        return self.half_step(half, probe_row, lo, hi, final=(part == 2))
+
+    def half_step(self, half, probe_row=None, lo=None, hi=None, final=True):
         ex, ey, ez, hx, hy, hz = self.f
         a, cb = self.a, self.cb
-        lo, hi = 1, self.nloc + 1                       # owned local planes
+        full = lo is None
+        if full:
+            lo, hi = 1, self.nloc + 1                   # owned local planes
         glob = lambda p: p + self.x0 - 1                 # noqa: E731
         if half == 0:
             L = slice(lo, hi)
@@ -94,8 +109,12 @@ class NumpySlabStepper:
             for c in (ex, ey, ez):
                 c[L] = c[L] * self.damp[L]
         flat = [c.reshape(-1) for c in (ex, ey, ez, hx, hy, hz)]
+        plane = self.shape[1] * self.shape[2]
         for cell, comp, amp, row in self.src:
-            flat[comp][cell] += amp * self.wave[row, self.step]
+            if lo <= cell // plane < hi:
+                flat[comp][cell] += amp * self.wave[row, self.step]
+        if not final:
+            return
         if probe_row is not None:
             for k, (cell, comp) in enumerate(self.probes):
                 probe_row[k] = float(flat[comp][cell])

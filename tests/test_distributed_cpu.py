@@ -29,7 +29,7 @@ def _sources(dt):
 PROBES = [(6, 5, 9, "ez"), (2, 8, 2, "hy"), (11, 3, 7, "ex"), (4, 4, 4, "hz")]
 
 
-def _worker(rank, world, port, boundary, out_path):
+def _worker(rank, world, port, boundary, out_path, overlap=True):
     import torch.distributed as dist
 
     from dist_helpers import NumpySlabStepper
@@ -39,7 +39,9 @@ def _worker(rank, world, port, boundary, out_path):
                             world_size=world)
     try:
         g = DistributedGrid3D(SIZE, resolution=1.0, boundary=boundary, pml_layers=3,
-                              stepper_factory=lambda **kw: NumpySlabStepper(**kw))
+                              stepper_factory=lambda **kw: NumpySlabStepper(**kw),
+                              overlap=overlap)
+        assert g.overlap == overlap
         for s in _sources(g.dt):
             g.add_source(s)
         for p in PROBES:
@@ -57,12 +59,16 @@ def _worker(rank, world, port, boundary, out_path):
 
 @pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("boundary", ["absorbing", "pec"])
-def test_slab_decomposition_matches_oracle(world, boundary):
+@pytest.mark.parametrize("overlap", [True, False])
+def test_slab_decomposition_matches_oracle(world, boundary, overlap):
+    """Both schedules: plain (exchange, then the whole half-step) and
+    overlapped (the neighbour's plane first, the exchange during the rest)."""
     from dist_helpers import free_port
 
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "r.npz")
-        mp.start_processes(_worker, args=(world, free_port(), boundary, out), nprocs=world,
+        mp.start_processes(_worker, args=(world, free_port(), boundary, out, overlap),
+                           nprocs=world,
                            join=True, start_method="spawn")
         res = np.load(out)
         dt = rn.default_dt_3d(1.0)

@@ -31,7 +31,7 @@ def _sources(dt):
                           waveform="gauss_sine", width_steps=5.0)]
 
 
-def _worker(rank, world, port, boundary, out_path):
+def _worker(rank, world, port, boundary, out_path, overlap=True):
     import torch
     import torch.distributed as dist
 
@@ -41,7 +41,8 @@ def _worker(rank, world, port, boundary, out_path):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world)
     try:
-        g = DistributedGrid3D(SIZE, resolution=1.0, boundary=boundary, pml_layers=4, device=0)
+        g = DistributedGrid3D(SIZE, resolution=1.0, boundary=boundary, pml_layers=4, device=0,
+                              overlap=overlap)
         for s in _sources(g.dt):
             g.add_source(s)
         for p in PROBES:
@@ -58,14 +59,17 @@ def _worker(rank, world, port, boundary, out_path):
 
 
 @pytest.mark.parametrize("world,boundary", [(2, "cpml"), (3, "absorbing"), (2, "pec")])
-def test_decomposed_run_equals_single_grid(cuda, world, boundary):
+@pytest.mark.parametrize("overlap", [True, False])
+def test_decomposed_run_equals_single_grid(cuda, world, boundary, overlap):
+    """Plain and overlapped (boundary plane first, exchange during the other
+    planes) schedules, bit for bit against the undecomposed grid."""
     from dist_helpers import free_port
     from jaxphys_b200 import EMGrid3D
 
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "r.npz")
-        mp.start_processes(_worker, args=(world, free_port(), boundary, out), nprocs=world,
-                           join=True, start_method="spawn")
+        mp.start_processes(_worker, args=(world, free_port(), boundary, out, overlap),
+                           nprocs=world, join=True, start_method="spawn")
         res = np.load(out)
         g = EMGrid3D(SIZE, resolution=1.0, boundary=boundary, pml_layers=4, path="generic")
         dt = g.default_dt()
