@@ -2321,7 +2321,7 @@ void batch_tma_kernel(const jxf_batch3d* b, int part, TmaBatchKernel* k, size_t*
 
 // One leapfrog step of a TMA batch: the parts' persistent launches chained by
 // programmatic dependent launch (capturable).
-int batch_tma_launch(jxf_batch3d* b, int in_set, cudaStream_t st) {
+int batch_tma_launch(jxf_batch3d* b, int in_set, long long step, cudaStream_t st) {
   const TmaConfig& c = tma_configs()[b->cfg];
   bool first = true;
   for (int pi = 0; pi < 5; ++pi) {
@@ -2337,6 +2337,7 @@ int batch_tma_launch(jxf_batch3d* b, int in_set, cudaStream_t st) {
     a.items = b->d_items + b->part_off[pi];
     a.n_items = b->part_n[pi];
     a.counter = b->d_counters + 2 * pi;
+    a.step = step;
     a.pdl = b->use_pdl ? (first ? (PDL_WAIT_START | PDL_TRIGGER) : (PDL_TRIGGER | PDL_WAIT_END))
                        : 0;
     cudaLaunchConfig_t lc{};
@@ -2578,7 +2579,7 @@ int batch_refresh(jxf_batch3d* b) {
 int batch_launch_step(jxf_batch3d* b, long long step, float* probe_row, cudaStream_t st,
                       int in_set = 0) {
   if (b->tma) {
-    TRY(batch_tma_launch(b, in_set, st));
+    TRY(batch_tma_launch(b, in_set, step, st));
     if (b->band.band) TRY(band_launch(b->band, st, in_set ^ 1));
     if (probe_row && b->n_probes > 0)
       k3d_batch_probes<<<(b->n_probes + 127) / 128, 128, 0, st>>>(
@@ -2642,11 +2643,11 @@ int batch_tma_tune(jxf_batch3d* b, int in_set, cudaStream_t st) {
         b->axis_split = sp;
         bool moved = false;
         TRY(batch_tma_tables(b, &moved));
-        TRY(batch_tma_launch(b, in_set, st));
+        TRY(batch_tma_launch(b, in_set, b->step, st));
         float ms = 1e30f;
         for (int trial = 0; trial < 2; ++trial) {
           CUDA_TRY(cudaEventRecord(e0, st));
-          for (int r = 0; r < 2; ++r) TRY(batch_tma_launch(b, in_set, st));
+          for (int r = 0; r < 2; ++r) TRY(batch_tma_launch(b, in_set, b->step, st));
           CUDA_TRY(cudaEventRecord(e1, st));
           CUDA_TRY(cudaEventSynchronize(e1));
           float t = 0;

@@ -568,7 +568,7 @@ __device__ __forceinline__ void slab_first_cell(int t, int z0, int y0, int nz, i
 // persistent block looping over the items of many grids).
 template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA, int AXES = 7>
 __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, int tzi, int tyi,
-                                          int ci, bool slab_first) {
+                                          int ci, bool slab_first, long long step) {
   constexpr bool CPML = (MODE == MODE_CPML);
   constexpr bool AX = (AXES & 1) != 0, AY = (AXES & 2) != 0, AZ = (AXES & 4) != 0;
   using L = TmaLayout<TZ, TY, RY, STAGES, CBARR, CPML, AXES>;
@@ -1035,7 +1035,7 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
         const int tz_e = e.off - yl_e * TZ;
         if (tz_e == tx && (yl_e % TYT) == ty) {
           const int r_e = yl_e / TYT;
-          const float v = fmul(e.amp, p.wave[(long long)e.wave * p.wave_len + p.step]);
+          const float v = fmul(e.amp, p.wave[(long long)e.wave * p.wave_len + step]);
 #pragma unroll
           for (int r = 0; r < RY; ++r) {
             if (r == r_e) {
@@ -1114,7 +1114,8 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
   // step, which waits on the interior kernel, also sees the shell's writes).
   if (p.pdl & PDL_WAIT_START) grid_dep_wait();
   if (p.pdl & PDL_TRIGGER) grid_dep_launch_dependents();
-  tma_block<TZ, TY, RY, STAGES, MODE, CBARR, KAPPA, AXES>(p, maps, tzi, tyi, ci, slab_first);
+  tma_block<TZ, TY, RY, STAGES, MODE, CBARR, KAPPA, AXES>(p, maps, tzi, tyi, ci, slab_first,
+                                                          p.step);
   if (p.pdl & PDL_WAIT_END) grid_dep_wait();
 }
 
@@ -1132,6 +1133,7 @@ struct TmaBatchArgs {
   int n_items;
   int* counter;          // [0] next item, [1] blocks done
   int pdl;
+  long long step;        // step index of the batch (waveform sample of the sources)
 };
 
 __device__ __forceinline__ void mbar_inval(uint64_t* bar) {
@@ -1168,7 +1170,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       if (CBARR) tensormap_acquire(&m.cb);
     }
     tma_block<TZ, TY, RY, STAGES, MODE, CBARR, KAPPA, AXES>(
-        a.params[k], m, w.y, w.z, w.w & BLK_CHUNK_MASK, (w.w & BLK_SLAB_FIRST) != 0);
+        a.params[k], m, w.y, w.z, w.w & BLK_CHUNK_MASK, (w.w & BLK_SLAB_FIRST) != 0, a.step);
     __syncthreads();  // every wait of the item is over
     if (threadIdx.x == 0)
       for (int s = 0; s < STAGES; ++s) mbar_inval(&bars[s]);

@@ -92,9 +92,18 @@ struct TbLayout {
   // warp edge buffers: XH1[2][NW][32], XE1[2 parity][2][NW][32], XH2[2][NW][32]
   static constexpr int X_FLOATS = 8 * NW * 32;
   static constexpr int NPSI = CPML ? psi_count(AXES) : 0;
-  static constexpr int PS_FLOATS = 2 * NPSI * NR * 32;  // psi^{n+1} by plane parity
-  static constexpr size_t SMEM_BYTES =
-      128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + X_FLOATS + PS_FLOATS);
+  // psi per thread and cell in shared memory.  Ring (when it fits): three
+  // slots by plane mod 3 -- psi^n of plane q+1 arrives by cp.async during
+  // march step q, level 1 of plane q turns its slot into psi^{n+1} in place,
+  // level 2 reads it one step later.  Otherwise two slots by plane parity
+  // hold psi^{n+1} and psi^n is read from global memory where it is used.
+  static constexpr size_t BASE_BYTES =
+      128 + sizeof(float) * ((size_t)STAGES * STAGE_FLOATS + X_FLOATS);
+  static constexpr bool RING =
+      CPML && BASE_BYTES + sizeof(float) * 3 * (size_t)NPSI * NR * 32 <= 227 * 1024;
+  static constexpr int NSLOT = RING ? 3 : 2;
+  static constexpr int PS_FLOATS = NSLOT * NPSI * NR * 32;
+  static constexpr size_t SMEM_BYTES = BASE_BYTES + sizeof(float) * (size_t)PS_FLOATS;
   static_assert(NR >= 8, "region too small");
   static_assert(STAGES >= 3 && STAGES <= 6, "ring needs >= 3 stages");
   static_assert(NT <= 1024, "block too large");
@@ -265,7 +274,44 @@ __global__ void __launch_bounds__(32 * NW)
       if (rin[k]) dyr[k] = __ldg(p.damp[1] + yv[k]);
   }
 
-#define PSV(par, id, k) PS[((((par) * L::NPSI + psi_slot(AXES, (id))) * NR) + r0 + (k)) * 32 + lane]
+#define PSV(slot, id, k) PS[((((slot) * L::NPSI + psi_slot(AXES, (id))) * NR) + r0 + (k)) * 32 + lane]
+// psi^n of a level-1 cell: from the ring slot, or from global memory
+#define PSN(id, off, k) (L::RING ? PSV(s1, id, k) : __ldg(p.pml.in[id] + (off)))
+  // cp.async of psi^n of plane qq (this thread's slab cells) into ring slot qq % 3
+  auto issue_psi = [&](int qq) {
+    const int sl = qq % 3;
+    const int imq = AX ? slab_map(qq, nx, p.pml.P[0]) : -1;
+#pragma unroll
+    for (int k = 0; k < RY; ++k) {
+      const bool valid = rin[k] && zin;
+      if (AY && iny[k]) {
+        const int o = qq * SY + oy[k];
+        cp_async4(&PSV(sl, PSI_HXY, k), p.pml.in[PSI_HXY] + o);
+        cp_async4(&PSV(sl, PSI_HZY, k), p.pml.in[PSI_HZY] + o);
+        cp_async4(&PSV(sl, PSI_EXY, k), p.pml.in[PSI_EXY] + o);
+        cp_async4(&PSV(sl, PSI_EZY, k), p.pml.in[PSI_EZY] + o);
+      }
+      if (AZ && inz && valid) {
+        const int o = qq * SZ + oz[k];
+        cp_async4(&PSV(sl, PSI_HXZ, k), p.pml.in[PSI_HXZ] + o);
+        cp_async4(&PSV(sl, PSI_HYZ, k), p.pml.in[PSI_HYZ] + o);
+        cp_async4(&PSV(sl, PSI_EXZ, k), p.pml.in[PSI_EXZ] + o);
+        cp_async4(&PSV(sl, PSI_EYZ, k), p.pml.in[PSI_EYZ] + o);
+      }
+      if (AX && imq >= 0 && valid) {
+        const int o = imq * SX + ox[k];
+        cp_async4(&PSV(sl, PSI_HYX, k), p.pml.in[PSI_HYX] + o);
+        cp_async4(&PSV(sl, PSI_HZX, k), p.pml.in[PSI_HZX] + o);
+        cp_async4(&PSV(sl, PSI_EYX, k), p.pml.in[PSI_EYX] + o);
+        cp_async4(&PSV(sl, PSI_EZX, k), p.pml.in[PSI_EZX] + o);
+      }
+    }
+  };
+  const int q1last = min(xe, nx - 1);  // last level-1 plane
+  if (L::RING) {
+    if (qs <= q1last) issue_psi(qs);
+    cp_async_commit();
+  }
 
   // source / probe lists of this block
   const int bid = (ci * p.ntiles_y + tyi) * p.ntiles_z + tzi;
@@ -316,6 +362,14 @@ __global__ void __launch_bounds__(32 * NW)
     const bool have_next = q + 1 <= ql;    // plane q+1 staged
     const int slot = l % STAGES;
     const int par = q & 1;
+    // psi slots: level 1 (plane q) and level 2 (plane q-1)
+    const int s1 = L::RING ? q % 3 : par;
+    const int s2 = L::RING ? (q + 2) % 3 : par ^ 1;
+    if (L::RING) {
+      if (q + 1 <= q1last) issue_psi(q + 1);
+      cp_async_commit();                 // (possibly empty) group of plane q+1
+      cp_async_wait_pending<1>();        // plane q's psi^n has landed
+    }
     bool ok = true;
     if (have_next) {
       ok = mbar_wait_bounded(&bars[(l + 1) % STAGES], (uint32_t)(((l + 1) / STAGES) & 1),
@@ -392,24 +446,24 @@ __global__ void __launch_bounds__(32 * NW)
         if (CPML && __any_sync(FULL, cy || cz || cx)) {
           const int oyq = q * SY + oy[k], ozq = q * SZ + oz[k], oxq = imq * SX + ox[k];
           if (ux) {
-            const float p1 = pnext(cy, ybh[k], ych[k], cy ? __ldg(p.pml.in[PSI_HXY] + oyq) : 0.f, dyEz);
-            const float p2 = pnext(cz, zbh, zch, cz ? __ldg(p.pml.in[PSI_HXZ] + ozq) : 0.f, dzEy);
-            if (cy) PSV(par, PSI_HXY, k) = p1;
-            if (cz) PSV(par, PSI_HXZ, k) = p2;
+            const float p1 = pnext(cy, ybh[k], ych[k], cy ? PSN(PSI_HXY, oyq, k) : 0.f, dyEz);
+            const float p2 = pnext(cz, zbh, zch, cz ? PSN(PSI_HXZ, ozq, k) : 0.f, dzEy);
+            if (cy) PSV(s1, PSI_HXY, k) = p1;
+            if (cz) PSV(s1, PSI_HXZ, k) = p2;
             hx = h_sel<KAPPA>(hx, a, dyEz, dzEy, cy, cz, p1, p2, yikh[k], zikh);
           }
           if (uy) {
-            const float p1 = pnext(cz, zbh, zch, cz ? __ldg(p.pml.in[PSI_HYZ] + ozq) : 0.f, dzEx);
-            const float p2 = pnext(cx, xbh, xch, cx ? __ldg(p.pml.in[PSI_HYX] + oxq) : 0.f, dxEz);
-            if (cz) PSV(par, PSI_HYZ, k) = p1;
-            if (cx) PSV(par, PSI_HYX, k) = p2;
+            const float p1 = pnext(cz, zbh, zch, cz ? PSN(PSI_HYZ, ozq, k) : 0.f, dzEx);
+            const float p2 = pnext(cx, xbh, xch, cx ? PSN(PSI_HYX, oxq, k) : 0.f, dxEz);
+            if (cz) PSV(s1, PSI_HYZ, k) = p1;
+            if (cx) PSV(s1, PSI_HYX, k) = p2;
             hy = h_sel<KAPPA>(hy, a, dzEx, dxEz, cz, cx, p1, p2, zikh, xikh);
           }
           if (uz) {
-            const float p1 = pnext(cx, xbh, xch, cx ? __ldg(p.pml.in[PSI_HZX] + oxq) : 0.f, dxEy);
-            const float p2 = pnext(cy, ybh[k], ych[k], cy ? __ldg(p.pml.in[PSI_HZY] + oyq) : 0.f, dyEx);
-            if (cx) PSV(par, PSI_HZX, k) = p1;
-            if (cy) PSV(par, PSI_HZY, k) = p2;
+            const float p1 = pnext(cx, xbh, xch, cx ? PSN(PSI_HZX, oxq, k) : 0.f, dxEy);
+            const float p2 = pnext(cy, ybh[k], ych[k], cy ? PSN(PSI_HZY, oyq, k) : 0.f, dyEx);
+            if (cx) PSV(s1, PSI_HZX, k) = p1;
+            if (cy) PSV(s1, PSI_HZY, k) = p2;
             hz = h_sel<KAPPA>(hz, a, dxEy, dyEx, cx, cy, p1, p2, xikh, yikh[k]);
           }
         } else {
@@ -459,24 +513,24 @@ __global__ void __launch_bounds__(32 * NW)
         if (CPML && __any_sync(FULL, cy || cz || cx)) {
           const int oyq = q * SY + oy[k], ozq = q * SZ + oz[k], oxq = imq * SX + ox[k];
           if (ux) {
-            const float p1 = pnext(cy, ybe[k], yce[k], cy ? __ldg(p.pml.in[PSI_EXY] + oyq) : 0.f, dyHz);
-            const float p2 = pnext(cz, zbe, zce, cz ? __ldg(p.pml.in[PSI_EXZ] + ozq) : 0.f, dzHy);
-            if (cy) PSV(par, PSI_EXY, k) = p1;
-            if (cz) PSV(par, PSI_EXZ, k) = p2;
+            const float p1 = pnext(cy, ybe[k], yce[k], cy ? PSN(PSI_EXY, oyq, k) : 0.f, dyHz);
+            const float p2 = pnext(cz, zbe, zce, cz ? PSN(PSI_EXZ, ozq, k) : 0.f, dzHy);
+            if (cy) PSV(s1, PSI_EXY, k) = p1;
+            if (cz) PSV(s1, PSI_EXZ, k) = p2;
             exv = e_sel<KAPPA>(exv, cb, dyHz, dzHy, cy, cz, p1, p2, yike[k], zike);
           }
           if (uy) {
-            const float p1 = pnext(cz, zbe, zce, cz ? __ldg(p.pml.in[PSI_EYZ] + ozq) : 0.f, dzHx);
-            const float p2 = pnext(cx, xbe, xce, cx ? __ldg(p.pml.in[PSI_EYX] + oxq) : 0.f, dxHz);
-            if (cz) PSV(par, PSI_EYZ, k) = p1;
-            if (cx) PSV(par, PSI_EYX, k) = p2;
+            const float p1 = pnext(cz, zbe, zce, cz ? PSN(PSI_EYZ, ozq, k) : 0.f, dzHx);
+            const float p2 = pnext(cx, xbe, xce, cx ? PSN(PSI_EYX, oxq, k) : 0.f, dxHz);
+            if (cz) PSV(s1, PSI_EYZ, k) = p1;
+            if (cx) PSV(s1, PSI_EYX, k) = p2;
             eyv = e_sel<KAPPA>(eyv, cb, dzHx, dxHz, cz, cx, p1, p2, zike, xike);
           }
           if (uz) {
-            const float p1 = pnext(cx, xbe, xce, cx ? __ldg(p.pml.in[PSI_EZX] + oxq) : 0.f, dxHy);
-            const float p2 = pnext(cy, ybe[k], yce[k], cy ? __ldg(p.pml.in[PSI_EZY] + oyq) : 0.f, dyHx);
-            if (cx) PSV(par, PSI_EZX, k) = p1;
-            if (cy) PSV(par, PSI_EZY, k) = p2;
+            const float p1 = pnext(cx, xbe, xce, cx ? PSN(PSI_EZX, oxq, k) : 0.f, dxHy);
+            const float p2 = pnext(cy, ybe[k], yce[k], cy ? PSN(PSI_EZY, oyq, k) : 0.f, dyHx);
+            if (cx) PSV(s1, PSI_EZX, k) = p1;
+            if (cy) PSV(s1, PSI_EZY, k) = p2;
             ezv = e_sel<KAPPA>(ezv, cb, dxHy, dyHx, cx, cy, p1, p2, xike, yike[k]);
           }
         } else {
@@ -575,22 +629,22 @@ __global__ void __launch_bounds__(32 * NW)
           const bool own = own_plane && trow[k] && tlane;
           const int oyq = x2 * SY + oy[k], ozq = x2 * SZ + oz[k], oxq = imp * SX + ox[k];
           if (ux) {
-            const float p1 = pnext(cy, ybh[k], ych[k], cy ? PSV(ppar, PSI_HXY, k) : 0.f, dyEz);
-            const float p2 = pnext(cz, zbh, zch, cz ? PSV(ppar, PSI_HXZ, k) : 0.f, dzEy);
+            const float p1 = pnext(cy, ybh[k], ych[k], cy ? PSV(s2, PSI_HXY, k) : 0.f, dyEz);
+            const float p2 = pnext(cz, zbh, zch, cz ? PSV(s2, PSI_HXZ, k) : 0.f, dzEy);
             if (own && cy) p.pml.out[PSI_HXY][oyq] = p1;
             if (own && cz) p.pml.out[PSI_HXZ][ozq] = p2;
             hx = h_sel<KAPPA>(hx, a, dyEz, dzEy, cy, cz, p1, p2, yikh[k], zikh);
           }
           if (uy) {
-            const float p1 = pnext(cz, zbh, zch, cz ? PSV(ppar, PSI_HYZ, k) : 0.f, dzEx);
-            const float p2 = pnext(cx, pbh, pch, cx ? PSV(ppar, PSI_HYX, k) : 0.f, dxEz);
+            const float p1 = pnext(cz, zbh, zch, cz ? PSV(s2, PSI_HYZ, k) : 0.f, dzEx);
+            const float p2 = pnext(cx, pbh, pch, cx ? PSV(s2, PSI_HYX, k) : 0.f, dxEz);
             if (own && cz) p.pml.out[PSI_HYZ][ozq] = p1;
             if (own && cx) p.pml.out[PSI_HYX][oxq] = p2;
             hy = h_sel<KAPPA>(hy, a, dzEx, dxEz, cz, cx, p1, p2, zikh, pikh);
           }
           if (uz) {
-            const float p1 = pnext(cx, pbh, pch, cx ? PSV(ppar, PSI_HZX, k) : 0.f, dxEy);
-            const float p2 = pnext(cy, ybh[k], ych[k], cy ? PSV(ppar, PSI_HZY, k) : 0.f, dyEx);
+            const float p1 = pnext(cx, pbh, pch, cx ? PSV(s2, PSI_HZX, k) : 0.f, dxEy);
+            const float p2 = pnext(cy, ybh[k], ych[k], cy ? PSV(s2, PSI_HZY, k) : 0.f, dyEx);
             if (own && cx) p.pml.out[PSI_HZX][oxq] = p1;
             if (own && cy) p.pml.out[PSI_HZY][oyq] = p2;
             hz = h_sel<KAPPA>(hz, a, dxEy, dyEx, cx, cy, p1, p2, pikh, yikh[k]);
@@ -618,7 +672,6 @@ __global__ void __launch_bounds__(32 * NW)
 
     // ================= level 2: E^{n+2}(q-1), stores =================
     if (lvl2h && x2 >= xb) {
-      const int ppar = x2 & 1;
       const bool inx = AX && imp >= 0;
       const float dxq = MODE == MODE_ABSORB ? __ldg(p.damp[0] + x2) : 1.f;
       float eo[3][RY];
@@ -646,22 +699,22 @@ __global__ void __launch_bounds__(32 * NW)
           const bool own = trow[k] && tlane;
           const int oyq = x2 * SY + oy[k], ozq = x2 * SZ + oz[k], oxq = imp * SX + ox[k];
           if (ux) {
-            const float p1 = pnext(cy, ybe[k], yce[k], cy ? PSV(ppar, PSI_EXY, k) : 0.f, dyHz);
-            const float p2 = pnext(cz, zbe, zce, cz ? PSV(ppar, PSI_EXZ, k) : 0.f, dzHy);
+            const float p1 = pnext(cy, ybe[k], yce[k], cy ? PSV(s2, PSI_EXY, k) : 0.f, dyHz);
+            const float p2 = pnext(cz, zbe, zce, cz ? PSV(s2, PSI_EXZ, k) : 0.f, dzHy);
             if (own && cy) p.pml.out[PSI_EXY][oyq] = p1;
             if (own && cz) p.pml.out[PSI_EXZ][ozq] = p2;
             exv = e_sel<KAPPA>(exv, cb, dyHz, dzHy, cy, cz, p1, p2, yike[k], zike);
           }
           if (uy) {
-            const float p1 = pnext(cz, zbe, zce, cz ? PSV(ppar, PSI_EYZ, k) : 0.f, dzHx);
-            const float p2 = pnext(cx, pbe, pce, cx ? PSV(ppar, PSI_EYX, k) : 0.f, dxHz);
+            const float p1 = pnext(cz, zbe, zce, cz ? PSV(s2, PSI_EYZ, k) : 0.f, dzHx);
+            const float p2 = pnext(cx, pbe, pce, cx ? PSV(s2, PSI_EYX, k) : 0.f, dxHz);
             if (own && cz) p.pml.out[PSI_EYZ][ozq] = p1;
             if (own && cx) p.pml.out[PSI_EYX][oxq] = p2;
             eyv = e_sel<KAPPA>(eyv, cb, dzHx, dxHz, cz, cx, p1, p2, zike, pike);
           }
           if (uz) {
-            const float p1 = pnext(cx, pbe, pce, cx ? PSV(ppar, PSI_EZX, k) : 0.f, dxHy);
-            const float p2 = pnext(cy, ybe[k], yce[k], cy ? PSV(ppar, PSI_EZY, k) : 0.f, dyHx);
+            const float p1 = pnext(cx, pbe, pce, cx ? PSV(s2, PSI_EZX, k) : 0.f, dxHy);
+            const float p2 = pnext(cy, ybe[k], yce[k], cy ? PSV(s2, PSI_EZY, k) : 0.f, dyHx);
             if (own && cx) p.pml.out[PSI_EZX][oxq] = p1;
             if (own && cy) p.pml.out[PSI_EZY][oyq] = p2;
             ezv = e_sel<KAPPA>(ezv, cb, dxHy, dyHx, cx, cy, p1, p2, pike, yike[k]);
@@ -734,6 +787,8 @@ __global__ void __launch_bounds__(32 * NW)
 #undef HS
   }
 #undef PSV
+#undef PSN
+  if (L::RING) cp_async_wait_all();
 
   if (aborted) {
     // A staged copy never arrived.  Record it, then wait (bounded) for every
