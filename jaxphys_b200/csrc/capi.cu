@@ -316,10 +316,10 @@ struct jxf_grid3d {
   int* d_tb_probe_ptr = nullptr;
   int tb_built_cfg = -1, tb_built_chunk = -1;
   int* d_tb_shell = nullptr;
-  int* d_tb_shell_ax[3] = {};
+  int* d_tb_shell_ax[6] = {};  // one axis (x, y, z), two axes (xy, xz, yz)
   int* d_tb_inner = nullptr;
   int n_tb_shell = 0, n_tb_inner = 0;
-  int n_tb_shell_ax[3] = {0, 0, 0};
+  int n_tb_shell_ax[6] = {0, 0, 0, 0, 0, 0};
   int tb_split_cfg = -1, tb_split_chunk = -1, tb_split_axes = -1;
 };
 
@@ -871,7 +871,7 @@ int build_tb_split(jxf_grid3d* g, int cfg, int chunk) {
   struct Blk {
     int cost, tz, ty, ch;
   };
-  std::vector<Blk> shell_b, axl_b[3];
+  std::vector<Blk> shell_b, axl_b[6];
   std::vector<int> inner;
   const bool axis_split = g->axis_split != 0;
   for (int ch = 0; ch < nch; ++ch)
@@ -894,6 +894,8 @@ int build_tb_split(jxf_grid3d* g, int cfg, int chunk) {
           xs += in_slab(x, nx, g->P[0]) ? 1 : 0;
         std::vector<Blk>* v = &shell_b;
         if (touched == 1 && !g->kappa && axis_split) v = &axl_b[!cx ? 0 : (!cy ? 1 : 2)];
+        // two axes: xy, xz, yz
+        if (touched == 2 && !g->kappa && axis_split) v = &axl_b[cz ? 3 : (cy ? 4 : 5)];
         v->push_back({touched * 4096 + xs, tz, ty, ch});
       }
   auto flatten = [&](std::vector<Blk>& in, std::vector<int>& out) {
@@ -906,12 +908,12 @@ int build_tb_split(jxf_grid3d* g, int cfg, int chunk) {
       out.push_back(b.ch);
     }
   };
-  std::vector<int> shell, axl[3];
+  std::vector<int> shell, axl[6];
   flatten(shell_b, shell);
-  for (int a = 0; a < 3; ++a) flatten(axl_b[a], axl[a]);
+  for (int a = 0; a < 6; ++a) flatten(axl_b[a], axl[a]);
   TRY(upload(&g->d_tb_shell, shell, &g->bytes));
   TRY(upload(&g->d_tb_inner, inner, &g->bytes));
-  for (int a = 0; a < 3; ++a) {
+  for (int a = 0; a < 6; ++a) {
     TRY(upload(&g->d_tb_shell_ax[a], axl[a], &g->bytes));
     g->n_tb_shell_ax[a] = (int)axl[a].size() / 3;
   }
@@ -933,9 +935,12 @@ int launch_tb(jxf_grid3d* g, int cfg, int chunk, Step3D& p, const TbExtra& ex, i
   const int ki = cpml ? (g->kappa ? 2 : 1) : 0;
   TbKernel k = c.k[ki][g->cb ? 1 : 0];
   size_t smem = c.smem[cpml ? 1 : 0];
-  if (cpml && axis >= 0) {
+  if (cpml && axis >= 0 && axis < 3) {
     k = c.kax[axis][g->cb ? 1 : 0];
     smem = c.smem_ax[axis];
+  } else if (cpml && axis >= 3) {
+    k = c.kax2[axis - 3][g->cb ? 1 : 0];
+    smem = c.smem_ax2[axis - 3];
   }
   {
     static std::mutex mu;
@@ -993,7 +998,10 @@ int launch_tb_step(jxf_grid3d* g, int cfg, int chunk, Step3D& p, const TbExtra& 
     bool plain;
     int axis;
   };
-  const Part parts[5] = {{g->d_tb_shell, g->n_tb_shell, false, -1},
+  const Part parts[8] = {{g->d_tb_shell, g->n_tb_shell, false, -1},
+                         {g->d_tb_shell_ax[3], g->n_tb_shell_ax[3], false, 3},
+                         {g->d_tb_shell_ax[4], g->n_tb_shell_ax[4], false, 4},
+                         {g->d_tb_shell_ax[5], g->n_tb_shell_ax[5], false, 5},
                          {g->d_tb_shell_ax[0], g->n_tb_shell_ax[0], false, 0},
                          {g->d_tb_shell_ax[1], g->n_tb_shell_ax[1], false, 1},
                          {g->d_tb_shell_ax[2], g->n_tb_shell_ax[2], false, 2},
@@ -1452,7 +1460,7 @@ int jxf_grid3d_destroy(jxf_grid3d* g) {
   dfree(g->d_tb_probe);
   dfree(g->d_tb_probe_ptr);
   dfree(g->d_tb_shell);
-  for (int a = 0; a < 3; ++a) dfree(g->d_tb_shell_ax[a]);
+  for (int a = 0; a < 6; ++a) dfree(g->d_tb_shell_ax[a]);
   dfree(g->d_tb_inner);
   dfree(g->adj_ck);
   dfree(g->adj_sg);
@@ -1497,7 +1505,8 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
             ? 1
             : (g->n_tb_shell > 0 ? 1 : 0) + (g->n_tb_inner > 0 ? 1 : 0) +
                   (g->n_tb_shell_ax[0] > 0 ? 1 : 0) + (g->n_tb_shell_ax[1] > 0 ? 1 : 0) +
-                  (g->n_tb_shell_ax[2] > 0 ? 1 : 0);
+                  (g->n_tb_shell_ax[2] > 0 ? 1 : 0) + (g->n_tb_shell_ax[3] > 0 ? 1 : 0) +
+                  (g->n_tb_shell_ax[4] > 0 ? 1 : 0) + (g->n_tb_shell_ax[5] > 0 ? 1 : 0);
   else
     out->blocked_kernels_per_pass = 0;
   if (g->path == JXF_PATH_GENERIC)

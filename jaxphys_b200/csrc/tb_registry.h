@@ -20,6 +20,8 @@ struct TbConfig {
   TbKernel k[3][2];   // [0 absorb, 1 cpml (kappa = 1), 2 cpml (kappa > 1)][cbarr]
   size_t smem_ax[3];  // CPML (kappa = 1) for blocks touching one axis's slab [x, y, z]
   TbKernel kax[3][2];
+  size_t smem_ax2[3];  // CPML (kappa = 1) for blocks touching two axes' slabs [xy, xz, yz]
+  TbKernel kax2[3][2];
 };
 
 const std::vector<TbConfig>& tb_configs();
