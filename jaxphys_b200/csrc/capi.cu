@@ -3002,6 +3002,11 @@ int band_launch(const BandTables& t, cudaStream_t st, int set) {
   a.delta = t.d_delta;
   a.err = t.band->d_err;
   a.wait_ns = wait_limit_ns();
+  {
+    // fault injection for tests (read at every launch): JXF_FAULT_DROP_MMA=1
+    const char* e = std::getenv("JXF_FAULT_DROP_MMA");
+    a.drop_first_mma = (e && e[0] == '1') ? 1 : 0;
+  }
   band::k_band_infer<band::SRC_GRIDS><<<t.ctas, 128, band::kInfSmem, st>>>(a);
   const int n = t.tiles * band::kTile;
   band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(grids, t.d_cells, n, t.d_delta);

@@ -243,6 +243,9 @@ struct InferArgs {
   const float* rows;          // SRC_ROWS: [n][54] normalised features
   int* err;
   unsigned long long wait_ns;
+  // fault injection for the failure-detection tests: every CTA leaves the
+  // first MMA of its first tile unissued, so its bounded waits run out
+  int drop_first_mma;
 };
 
 constexpr int kInfOffA = 0;        // activation image, 128 x 80
@@ -324,7 +327,7 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
       break;
     }
     // layer 1: Z1 = [X 1] [W1 b1]^T
-    if (tid == 0) {
+    if (tid == 0 && !(p.drop_first_mma && t == t0)) {
       tc::fence_after_sync();
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk)

@@ -50,7 +50,10 @@ const std::vector<TbConfig>& tb_configs() {
   static const std::vector<TbConfig> cfgs = {
       make_tb<4, 8, 3>(),   // 32-row region (29-row tile), 256 threads
       make_tb<2, 16, 3>(),  // 32-row region, 512 threads
-      make_tb<2, 8, 3>(),   // 16-row region (13-row tile), 256 threads: small grids
+      make_tb<2, 8, 3>(),   // 16-row region (13-row tile), 256 threads
+      make_tb<2, 12, 3>(),  // 24-row region (21-row tile), 384 threads
+      make_tb<1, 16, 3>(),  // 16-row region, one row per thread, 512 threads
+      make_tb<4, 4, 3>(),   // 16-row region, four rows per thread, 128 threads
   };
   return cfgs;
 }

@@ -16,7 +16,7 @@ from gpu_helpers import smooth_eps, to_np
 pytestmark = pytest.mark.gpu
 
 COMPS = ("ex", "ey", "ez", "hx", "hy", "hz")
-N_TB_CONFIGS = 3
+N_TB_CONFIGS = 6
 
 
 def _gauss(pos, pol="z", amp=1.0, width=10.0):

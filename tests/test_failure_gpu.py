@@ -9,6 +9,10 @@
   gets the generic kernel's result bit for bit: the GPU still answers.  Runs
   in a child process so the short wait limit (read once per process) does
   not reach the other tests.
+* A tensor-core step that never completes: JXF_FAULT_DROP_MMA=1 leaves the
+  first MMA of every learned-band inference CTA unissued; the waits on its
+  commit run out, the kernel frees its tensor memory and returns, and
+  jxf_band_check_error reports JXF_ERR_TIMEOUT.
 * A device allocation that fails: JXF_FAULT_ALLOC_AFTER=n refuses the
   (n+1)-th allocation of a grid creation; every such creation returns
   JXF_ERR_OOM, returns no handle and gives back what it had allocated.
@@ -115,3 +119,61 @@ def test_allocation_failure_leaves_nothing_behind(cuda, monkeypatch):
     # every refused creation freed what it had allocated (a field alone is
     # 3.5 MB; allow allocator slack)
     assert free0 - free1 < 16 << 20, (free0, free1)
+
+
+CHILD_BAND = textwrap.dedent("""
+    import os, sys
+    import numpy as np
+    sys.path.insert(0, {root!r})
+    from jaxphys_b200 import EMGrid3D, PointSource3D, SimulationError
+    from jaxphys_b200.em.batch import FDTDBatch
+    from jaxphys_b200.em.learned import default_band
+
+    def make():
+        grids = []
+        for i, size in enumerate(((24, 20, 28), (30, 26, 32))):
+            g = EMGrid3D(size=size, resolution=1.0, boundary="pec", path="tma")
+            g.add_source(PointSource3D(frequency=5e9, position=tuple(s // 2 for s in size)))
+            g.prepare()
+            grids.append(g)
+        b = FDTDBatch(grids)
+        b.set_band(default_band())
+        return grids, b
+
+    band = default_band()
+    grids, b = make()
+    os.environ["JXF_FAULT_DROP_MMA"] = "1"
+    b.run(1, use_graph=False)
+    try:
+        band.check()
+    except SimulationError as e:
+        assert "did not complete" in str(e), str(e)
+        print("band timeout reported")
+    else:
+        raise AssertionError("the dropped MMA was not reported")
+    del os.environ["JXF_FAULT_DROP_MMA"]
+    b.reset()
+    b.run(6, use_graph=False)
+    band.check()
+    ref_grids, ref = make()
+    ref.run(6, use_graph=False)
+    band.check()
+    for g, r in zip(grids, ref_grids):
+        for k in ("ex", "ey", "ez", "hx", "hy", "hz"):
+            assert np.array_equal(g.field(k).cpu().numpy(), r.field(k).cpu().numpy()), k
+    print("band recovered")
+""")
+
+
+def test_band_mma_timeout_reported_and_recovers(cuda):
+    """The learned band's tensor-core step: JXF_FAULT_DROP_MMA=1 leaves the
+    first MMA of every CTA's first tile unissued; the bounded waits run out,
+    the kernel frees its tensor memory and returns, jxf_band_check_error
+    reports JXF_ERR_TIMEOUT, and the next runs on the same GPU equal a fresh
+    batch bit for bit."""
+    env = dict(os.environ, JXF_WAIT_LIMIT_MS="200", JXF_AUTOTUNE="0")
+    env.pop("JXF_FAULT_DROP_MMA", None)
+    r = subprocess.run([sys.executable, "-c", CHILD_BAND.format(root=str(ROOT))], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "band timeout reported" in r.stdout and "band recovered" in r.stdout
