@@ -62,7 +62,11 @@ BAND_WEIGHTS = ROOT / "jaxphys_b200" / "em" / "band_weights.npz"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, ncu) per leapfrog
 # step of a workload, keyed by the launch shape they were captured at: a
 # figure applies only when the run's autotuned launch is that shape.
-NCU_TRAFFIC: dict = {}
+NCU_TRAFFIC: dict = {
+    # config 2 at registry entry 8 (64x4 tile, 3 stages), 16-plane chunks,
+    # single-axis split, one step per pass: general + z-only shell launches
+    ("c2", 8, 16, 1, -1, 0): 81.7e6,
+}
 
 
 def ncu_traffic(workload: str, launch: dict):
