@@ -52,6 +52,9 @@ WORKLOADS = {
     # config 3 at 256^3: the size the kernel profiles are captured at (fields
     # and psi ~1 GB, above L2, small enough for multi-pass ncu captures)
     "c3s": (256, 200, 12, "fdtd3d-256^3-cpml12-smoothnoise-eps1to12"),
+    # differentiable inverse design: forward with sqrt(T) checkpoints and the
+    # adjoint (time-reversed Yee) backward, dJ/d theta of 32^3 design cells
+    "c4": (96, 2000, 10, "adjoint-96^3-cpml10-2000steps-design32-planeEx-z15-probe-z80"),
     # batched learned boundary: 64 grids, interior sides uniform in [48, 160]
     "c5": (64, 1000, 3, "batch64-sides48to160-eps1to6-dipoles-learnedband3-vs-cpml10"),
 }
@@ -540,6 +543,78 @@ def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=
     return line
 
 
+def run_adjoint(args, world, rank, local, pg, steps=None, warmup=None, emit=True):
+    """c4: one gradient evaluation of config 4 = a forward run of 2000 steps
+    keeping sqrt(T) checkpoints + the adjoint backward (recomputing each
+    segment from its checkpoint, then the transposed steps); value = forward
+    cell updates per second of the whole gradient evaluation."""
+    import torch
+
+    from jaxphys_b200 import CPMLSpec, EMGrid3D, PointSource3D
+
+    n_timed = args.steps if steps is None else steps
+    n_warm = args.warmup if warmup is None else warmup
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    n, nsteps, pml, wname = WORKLOADS["c4"]
+    g = EMGrid3D(size=(n, n, n), resolution=1.0, boundary="cpml", pml_layers=pml,
+                 cpml=CPMLSpec(), device=local)
+    dt = g.default_dt()
+    for i in range(n):  # plane-wave Ex source at z = 15
+        for j in range(n):
+            g.add_source(PointSource3D(frequency=0.05 / dt, position=(i, j, 15), polarization="x",
+                                       waveform="gauss_sine", width_steps=30.0))
+    g.add_probe((n // 2, n // 2, 80), "ez")
+    g.prepare(dt=dt)
+    rng = np.random.default_rng(4 + rank)
+    theta = torch.tensor(rng.standard_normal((32, 32, 32)), dtype=torch.float32, device=dev)
+    eps = torch.ones((n, n, n), dtype=torch.float32, device=dev)
+    eps[32:64, 32:64, 32:64] = 1.0 + 11.0 * torch.sigmoid(theta)
+    g.set_permittivity_device(eps)
+    stream = torch.cuda.current_stream()
+
+    def one():
+        tr = g.adjoint_forward(nsteps)
+        grad = g.adjoint_backward(2.0 * tr)  # J = sum of squared probe values
+        return grad
+
+    for _ in range(max(n_warm, 1)):
+        one()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(n_timed)]
+    for k in range(n_timed):
+        ev[k][0].record(stream)
+        one()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    g.check()
+    ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    if pg is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n ** 3 * nsteps * n_timed * world / (ms * 1e-3) / 1e9
+    line = {
+        "metric": "adjoint gradient evaluation, forward Gcell-updates/s",
+        "value": round(value, 3), "unit": "Gcell/s", "n_gpus": world, "steps": n_timed,
+        "warmup": n_warm, "ms_per_step": round(ms / n_timed, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (dJ/dcb accumulated in f64)",
+        "data": "synthetic (seeded theta ~ N(0,1) on the central 32^3 cells)",
+        "config": {"workload": wname, "cells": n ** 3, "leapfrog_steps": nsteps,
+                   "checkpoints": "every ceil(sqrt(T)) steps",
+                   "note": "a gradient = forward + segment recompute + transposed steps"},
+        "gpu_launches": None, "clocks": clocks,
+    }
+    g._release()
+    if rank == 0 and emit:
+        print(json.dumps(line), flush=True)
+    return line
+
+
 def cpu_baseline(workload: str, budget_s: float = 10.0, steps: int | None = None):
     """The FP64 C restatement of the reference step on every host thread, on a
     bounded sample (a prefix of the workload's leapfrog steps)."""
@@ -580,10 +655,10 @@ def run_reference(args, world, rank):
     their total time."""
     if rank != 0:
         return
-    if args.workload == "c5":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference has neither a "
-                          "learned boundary nor batched grids; its CPU Yee path is timed under "
-                          "the c1/c2/c3 workloads"}), flush=True)
+    if args.workload in ("c4", "c5"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has neither an "
+                          "FDTD gradient nor a learned boundary or batched grids; its CPU Yee "
+                          "path is timed under the c1/c2/c3 workloads"}), flush=True)
         return
     n, nsteps, pml, wname = WORKLOADS[args.workload]
     budget = float(os.environ.get("JXF_REF_STEP_SECONDS", "12"))
@@ -625,9 +700,11 @@ def run_reference(args, world, rank):
 
 
 def secondary(args, world, rank, local, pg):
-    """Config 3 (512^3, 12-cell CPML, eps_r in [1, 12]) and config 5 (64
-    batched grids, learned band against CPML) measured in the same run as the
-    headline line, with their own short step counts (3 and 2 timed steps)."""
+    """Config 3 (512^3, 12-cell CPML, eps_r in [1, 12]), config 5 (64
+    batched grids, learned band against CPML) and config 4 (adjoint gradient
+    of the 96^3 inverse-design problem) measured in the same run as the
+    headline line, with their own short step counts (3, 2 and 2 timed
+    steps)."""
     out = {}
     c3 = run_ours(args, world, rank, local, pg, workload="c3", steps=3, warmup=1,
                   with_cpu=False, emit=False)
@@ -640,6 +717,9 @@ def secondary(args, world, rank, local, pg):
                                     "speedup_vs_cpml4_equal_error", "reflection_db",
                                     "roofline", "gpu_launches", "clocks", "dtype")}
     out["c5"]["config"] = c5["config"]
+    c4 = run_adjoint(args, world, rank, local, pg, steps=2, warmup=1, emit=False)
+    out["c4"] = {k: c4[k] for k in ("metric", "value", "unit", "ms_per_step", "steps", "warmup",
+                                    "clocks", "config")}
     return out
 
 
@@ -663,6 +743,8 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "c5":
             run_batch(args, world, rank, local, pg)
+        elif args.workload == "c4":
+            run_adjoint(args, world, rank, local, pg)
         elif args.workload == "c2" and world == 1 and not args.no_secondary:
             line = run_ours(args, world, rank, local, pg, emit=False)
             line["secondary"] = secondary(args, world, rank, local, pg)
