@@ -281,8 +281,6 @@ struct jxf_grid3d {
   // kernel, the others the plain kernel (compact block lists per launch shape)
   int* d_shell = nullptr;     // shell blocks touching slabs of several axes
   int* d_shell_ax[3] = {};    // shell blocks touching the slab of one axis (x, y, z)
-  int* d_shell_ax2[3] = {};   // shell blocks touching the slabs of two axes (xy, xz, yz)
-  int n_shell_ax2[3] = {0, 0, 0};
   int* d_inner = nullptr;
   int n_shell = 0, n_inner = 0;
   int n_shell_ax[3] = {0, 0, 0};
@@ -505,12 +503,9 @@ int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStr
   const int ki = cpml ? (g->kappa ? 2 : 1) : 0;
   TmaKernel k = c.k[ki][g->cb ? 1 : 0];
   size_t smem = c.smem[mi];
-  if (cpml && axis >= 0 && axis < 3) {  // single-axis shell blocks (kappa = 1 only)
+  if (cpml && axis >= 0) {  // single-axis shell blocks (kappa = 1 only)
     k = c.kax[axis][g->cb ? 1 : 0];
     smem = c.smem_ax[axis];
-  } else if (cpml && axis >= 3) {  // two-axis shell blocks (xy, xz, yz)
-    k = c.kax2[axis - 3][g->cb ? 1 : 0];
-    smem = c.smem_ax2[axis - 3];
   }
   {
     // the shared-memory opt-in is set once per kernel and device (a driver
@@ -628,15 +623,11 @@ double shell_block_cost(const jxf_grid3d* g, const TmaConfig& c, int cw, int xb,
 // slabs of several axes, of one axis (x, y, z), and interior blocks, each as
 // (tile_z, tile_y, chunk word) triples with a work estimate, heaviest first.
 struct SplitLists {
-  // [0 shell, 1..3 single-axis x/y/z, 4 interior, 5..7 two-axis xy/xz/yz]
-  std::vector<int> list[8];
-  std::vector<double> cost[8];  // per block
+  std::vector<int> list[5];     // [0 shell, 1..3 single-axis x/y/z, 4 interior]
+  std::vector<double> cost[5];  // per block
 };
 
-// pairs: blocks touching the slabs of exactly two axes get parts 5..7 (else
-// they join the shell of several axes)
-void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, SplitLists& out,
-                   bool pairs = false) {
+void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, SplitLists& out) {
   const TmaConfig& c = tma_configs()[cfg];
   const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
   const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
@@ -645,7 +636,7 @@ void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, Spl
     double cost;
     int tz, ty, word;
   };
-  std::vector<Blk> parts[8];
+  std::vector<Blk> parts[5];
   std::vector<int> tile_cw((size_t)ntz * nty, -1);  // filled on first use
   const int warps = (c.threads + 31) / 32;
   for (int ch = 0; ch < nch; ++ch)
@@ -664,7 +655,6 @@ void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, Spl
         }
         int pi = 0;
         if (touched == 1 && !g->kappa && axis_split) pi = 1 + (!cx ? 0 : (!cy ? 1 : 2));
-        if (touched == 2 && !g->kappa && axis_split && pairs) pi = 5 + (cz ? 0 : (cy ? 1 : 2));
         // blocks holding z-slab cells order them first (one row per thread)
         const bool slab_first = !cz && c.ry == 1 && slab_first_enabled();
         int& cw = tile_cw[(size_t)ty * ntz + tz];
@@ -672,8 +662,8 @@ void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, Spl
         parts[pi].push_back({shell_block_cost(g, c, cw, xb, xe), tz, ty,
                              ch | (slab_first ? BLK_SLAB_FIRST : 0)});
       }
-  for (int k = 0; k < 8; ++k) {
-    if (k != 4 && heavy_first_enabled())
+  for (int k = 0; k < 5; ++k) {
+    if (k < 4 && heavy_first_enabled())
       std::stable_sort(parts[k].begin(), parts[k].end(),
                        [](const Blk& u, const Blk& v) { return u.cost > v.cost; });
     out.list[k].clear();
@@ -691,14 +681,12 @@ int build_split(jxf_grid3d* g, int cfg, int chunk) {
   if (g->split_cfg == cfg && g->split_chunk == chunk && g->split_axes == g->axis_split)
     return JXF_OK;
   SplitLists sl;
-  compute_split(g, cfg, chunk, g->axis_split != 0, sl, true);
+  compute_split(g, cfg, chunk, g->axis_split != 0, sl);
   TRY(upload(&g->d_shell, sl.list[0], &g->bytes));
   TRY(upload(&g->d_inner, sl.list[4], &g->bytes));
   for (int a = 0; a < 3; ++a) {
     TRY(upload(&g->d_shell_ax[a], sl.list[1 + a], &g->bytes));
     g->n_shell_ax[a] = (int)sl.list[1 + a].size() / 3;
-    TRY(upload(&g->d_shell_ax2[a], sl.list[5 + a], &g->bytes));
-    g->n_shell_ax2[a] = (int)sl.list[5 + a].size() / 3;
   }
   g->n_shell = (int)sl.list[0].size() / 3;
   g->n_inner = (int)sl.list[4].size() / 3;
@@ -728,10 +716,7 @@ int launch_step(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaSt
     bool plain;
     int axis;
   };
-  const Part parts[8] = {{g->d_shell, g->n_shell, false, -1},
-                         {g->d_shell_ax2[0], g->n_shell_ax2[0], false, 3},
-                         {g->d_shell_ax2[1], g->n_shell_ax2[1], false, 4},
-                         {g->d_shell_ax2[2], g->n_shell_ax2[2], false, 5},
+  const Part parts[5] = {{g->d_shell, g->n_shell, false, -1},
                          {g->d_shell_ax[0], g->n_shell_ax[0], false, 0},
                          {g->d_shell_ax[1], g->n_shell_ax[1], false, 1},
                          {g->d_shell_ax[2], g->n_shell_ax[2], false, 2},
@@ -1469,7 +1454,6 @@ int jxf_grid3d_destroy(jxf_grid3d* g) {
   dfree(g->d_blk_ptr);
   dfree(g->d_shell);
   for (int a = 0; a < 3; ++a) dfree(g->d_shell_ax[a]);
-  for (int a = 0; a < 3; ++a) dfree(g->d_shell_ax2[a]);
   dfree(g->d_inner);
   dfree(g->d_tb_src);
   dfree(g->d_tb_src_ptr);
@@ -1509,8 +1493,7 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
     out->tile_z = out->tile_y = out->rows_per_thread = out->stages = out->x_chunk = 0;
   }
   out->device_bytes = g->bytes;
-  out->shell_blocks = g->n_shell + g->n_shell_ax[0] + g->n_shell_ax[1] + g->n_shell_ax[2] +
-                      g->n_shell_ax2[0] + g->n_shell_ax2[1] + g->n_shell_ax2[2];
+  out->shell_blocks = g->n_shell + g->n_shell_ax[0] + g->n_shell_ax[1] + g->n_shell_ax[2];
   out->interior_blocks = g->n_inner;
   out->tma_config = g->path == JXF_PATH_TMA ? g->cfg : -1;
   out->axis_split = g->axis_split;
@@ -1531,8 +1514,7 @@ int jxf_grid3d_get_info(const jxf_grid3d* g, jxf_grid3d_info* out) {
   else if (g->mode == MODE_CPML && g->split_cfg >= 0)
     out->kernels_per_step = (g->n_shell > 0 ? 1 : 0) + (g->n_inner > 0 ? 1 : 0) +
                             (g->n_shell_ax[0] > 0 ? 1 : 0) + (g->n_shell_ax[1] > 0 ? 1 : 0) +
-                            (g->n_shell_ax[2] > 0 ? 1 : 0) + (g->n_shell_ax2[0] > 0 ? 1 : 0) +
-                            (g->n_shell_ax2[1] > 0 ? 1 : 0) + (g->n_shell_ax2[2] > 0 ? 1 : 0);
+                            (g->n_shell_ax[2] > 0 ? 1 : 0);
   else
     out->kernels_per_step = 1;
   return JXF_OK;

@@ -31,15 +31,6 @@ TmaConfig make_cfg() {
   c.kax[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 2>;
   c.kax[2][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 4>;
   c.kax[2][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 4>;
-  c.smem_ax2[0] = TmaLayout<TZ, TY, RY, ST, true, true, 3>::SMEM_BYTES;
-  c.smem_ax2[1] = TmaLayout<TZ, TY, RY, ST, true, true, 5>::SMEM_BYTES;
-  c.smem_ax2[2] = TmaLayout<TZ, TY, RY, ST, true, true, 6>::SMEM_BYTES;
-  c.kax2[0][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 3>;
-  c.kax2[0][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 3>;
-  c.kax2[1][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 5>;
-  c.kax2[1][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 5>;
-  c.kax2[2][0] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, false, false, 6>;
-  c.kax2[2][1] = k3d_tma<TZ, TY, RY, ST, MODE_CPML, true, false, 6>;
   if constexpr (BATCH) {
     c.kb[0][0] = k3d_tma_batch<TZ, TY, RY, ST, MODE_ABSORB, false, false>;
     c.kb[0][1] = k3d_tma_batch<TZ, TY, RY, ST, MODE_ABSORB, true, false>;

@@ -20,9 +20,6 @@ struct TmaConfig {
   // CPML (kappa = 1) for blocks touching the slab of one axis only [x, y, z][cbarr]
   size_t smem_ax[3];
   TmaKernel kax[3][2];
-  // CPML (kappa = 1) for blocks touching the slabs of two axes [xy, xz, yz][cbarr]
-  size_t smem_ax2[3];
-  TmaKernel kax2[3][2];
   // persistent batch kernels (same indices; nullptr: shape not offered for batches)
   TmaBatchKernel kb[3][2];
   TmaBatchKernel kbax[3][2];
