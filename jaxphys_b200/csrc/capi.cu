@@ -1689,7 +1689,9 @@ int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stre
       set_io(g, p, g->cur, 1 - g->cur);
       p.step = g->step;
       p.probe_out = (probe_out && np > 0 && k >= 1) ? probe_out + (size_t)(k - 1) * np : nullptr;
-      if (g->tb >= 0 && n_steps - k >= 2) {
+      // (a learned band corrects the state between every two steps, so its
+      // grids take one step per pass)
+      if (g->tb >= 0 && !g->band.band && n_steps - k >= 2) {
         // two steps in one pass; the state after the first is recorded by
         // the probe cells' owner blocks
         const TbExtra ex = tb_extra(g, (probe_out && np > 0) ? probe_out + (size_t)k * np : nullptr);
@@ -1703,6 +1705,7 @@ int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stre
       g->cur ^= 1;
       g->step++;
       ++k;
+      if (g->band.band) TRY(band_launch(g->band, st, g->cur));
     }
     if (probe_out && np > 0) TRY(gather_probes(g, g->cur, probe_out + (size_t)(n_steps - 1) * np, st));
   } else {
@@ -2707,8 +2710,6 @@ extern "C" int jxf_batch3d_create(int32_t n, jxf_grid3d* const* grids, jxf_batch
                     "grid %d: TMA batches need a permittivity map on every grid or on none", i);
       if (g->kappa != grids[0]->kappa)
         return fail(JXF_ERR_INVALID, "grid %d: TMA batches share the CPML kappa grading", i);
-      if (g->band.band)
-        return fail(JXF_ERR_INVALID, "grid %d: attach the band to the batch, not the grid", i);
     }
   }
   DeviceGuard dg(dev);
@@ -3531,8 +3532,7 @@ int jxf_grid3d_set_band(jxf_grid3d* g, jxf_band* m) {
   CUDA_TRY(cudaDeviceSynchronize());
   band_release(g->band);
   if (!m) return JXF_OK;
-  if (g->path != JXF_PATH_GENERIC || g->slab)
-    return fail(JXF_ERR_INVALID, "a learned band runs on the generic path of a whole grid");
+  if (g->slab) return fail(JXF_ERR_INVALID, "a learned band runs on a whole grid");
   std::vector<jxf_grid3d*> one{g};
   return band_attach(one, m, g->d.device, &g->bytes, g->band);
 }

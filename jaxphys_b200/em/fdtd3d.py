@@ -138,7 +138,8 @@ class EMGrid3D:
         boundary: "absorbing" (reference damping layers), "periodic",
             "pec" (no boundary treatment), "cpml" (extension) or "learned"
             (extension: the outer 3 cell layers are a learned absorbing band,
-            ``jaxphys_b200.em.learned``; generic kernel path).
+            ``jaxphys_b200.em.learned``, applied after every step on either
+            kernel path).
         pml_layers: Number of damping / CPML layers.
         cpml: CPML grading (boundary="cpml").
         device: CUDA device ordinal (default: torch's current device).
@@ -171,7 +172,7 @@ class EMGrid3D:
         self._probes: list[tuple[int, int, int, int]] = []
         self._cpml = cpml or CPMLSpec()
         self._device = device
-        self._path = "generic" if boundary == "learned" else path
+        self._path = path
         self._band = band
         self._h = None
         self._h_key = None

@@ -255,6 +255,44 @@ def test_learned_boundary_grid_matches_batch(cuda):
     assert torch.isfinite(h.ey).all()
 
 
+def test_learned_boundary_on_tma_path(cuda):
+    """A learned-band grid on the TMA kernel (the band corrects the buffer set
+    each step wrote; one step per pass) equals the same grid on the generic
+    kernels bit for bit, and a TMA batch of it equals both."""
+    import torch
+
+    from jaxphys_b200 import EMGrid3D, PointSource3D
+    from jaxphys_b200.em.batch import FDTDBatch
+    from jaxphys_b200.em.fdtd3d import COMPONENTS
+
+    def make(path):
+        g = EMGrid3D((22, 20, 24), resolution=1.0, boundary="learned", path=path)
+        dt = g.default_dt()
+        g.add_source(PointSource3D(frequency=0.05 / dt, position=(11, 10, 12), polarization="z",
+                                   waveform="gauss_sine", width_steps=12.0))
+        g.add_probe((4, 5, 6), "ez")
+        g.add_probe((18, 2, 20), "hx")
+        g.prepare()
+        return g
+
+    a = make("tma")
+    assert a.info()["path"] == 2
+    ta = a.run(81)
+    b = make("generic")
+    tb = b.run(81)
+    assert torch.equal(ta, tb)
+    for c in COMPONENTS:
+        assert torch.equal(a.field(c), b.field(c)), c
+    c = make("tma")
+    bc = FDTDBatch([c])
+    assert bc.path == "tma"
+    tc = bc.run(81, use_graph=True)[0]
+    assert torch.equal(tc, tb)
+    for k in COMPONENTS:
+        assert torch.equal(c.field(k), b.field(k)), k
+    bc.close()
+
+
 def test_band_destroy_refused_while_attached(cuda):
     from jaxphys_b200 import EMGrid3D
     from jaxphys_b200.em.batch import FDTDBatch
