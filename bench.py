@@ -68,7 +68,7 @@ BAND_WEIGHTS = ROOT / "jaxphys_b200" / "em" / "band_weights.npz"
 NCU_TRAFFIC: dict = {
     # config 2 at registry entry 8 (64x4 tile, 3 stages), 16-plane chunks,
     # single-axis split, one step per pass: general + z-only shell launches
-    ("c2", 8, 16, 1, -1, 0): 81.7e6,
+    ("c2", 8, 16, 1, -1, 0): 80.7e6,
     # config 3 at 256^3, blocked passes of registry entry 2, 32-plane chunks,
     # one-step entry 8: the eight launches of a pass / 2
     ("c3s", 8, 32, 1, 2, 32): 610.7e6,
