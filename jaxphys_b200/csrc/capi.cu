@@ -3010,7 +3010,8 @@ int band_launch(const BandTables& t, cudaStream_t st, int set) {
   }
   band::k_band_infer<band::SRC_GRIDS><<<t.ctas, 128, band::kInfSmem, st>>>(a);
   const int n = t.tiles * band::kTile;
-  band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(grids, t.d_cells, n, t.d_delta);
+  band::k_band_apply<<<(n + 255) / 256, 256, 0, st>>>(grids, t.d_cells, n, t.d_delta,
+                                                      t.band->d_err);
   CUDA_TRY(cudaGetLastError());
   return JXF_OK;
 }

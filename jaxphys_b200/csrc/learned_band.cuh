@@ -130,12 +130,14 @@ __device__ __forceinline__ void init_hidden_tail(unsigned char* img, int tid, in
   }
 }
 
-// Raw stencil of an outer cell (v[54], H scaled by eta0); returns s.
+// Raw stencil of an outer cell (v[54], H scaled by eta0); returns s.  ctr
+// receives the cell's own six components as stored (unscaled).
 // Every load is issued before any value is used: positions outside the grid
 // along the tangent are loaded from the clamped (in-grid) neighbour and then
 // replaced by zero, so no load sits behind a branch and a thread keeps all
 // 54 (x, y faces) or 18 (z faces) loads in flight at once.
-__device__ __forceinline__ float gather(const GridRef& gref, int cell, int face, float* v) {
+__device__ __forceinline__ float gather(const GridRef& gref, int cell, int face, float* v,
+                                        float* ctr) {
   const GridRef g = gref;
   const int a = face >> 1, side = face & 1;
   float ss = 0.0f;
@@ -152,6 +154,8 @@ __device__ __forceinline__ float gather(const GridRef& gref, int cell, int face,
       for (int comp = 0; comp < 6; ++comp)
         q[w][comp] = __ldg(reinterpret_cast<const float4*>(g.f[comp] + row + (xw - x) * sx));
     }
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) ctr[comp] = side ? q[1][comp].w : q[1][comp].x;
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
       const bool in = x + w - 1 >= 0 && x + w - 1 < g.nx;
@@ -192,6 +196,8 @@ __device__ __forceinline__ float gather(const GridRef& gref, int cell, int face,
     }
   }
 #pragma unroll
+  for (int comp = 0; comp < 6; ++comp) ctr[comp] = raw[0][1][comp];
+#pragma unroll
   for (int l = 0; l < 3; ++l) {
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
@@ -230,6 +236,8 @@ __device__ __forceinline__ bool wait_all(uint64_t* bar, uint32_t phase, unsigned
 // range of tiles and reloads the face's weights when the face changes.  One
 // activation image (X, then G1, then G2; each MMA has completed before the
 // next epilogue overwrites it) and 64 TMEM columns (Z1, then Z2, then O).
+// The launch bound keeps 5 CTAs per SM (<= 102 registers), the residency
+// that shared memory and TMEM allow and that the grid is sized for.
 enum InferSrc : int { SRC_GRIDS = 0, SRC_ROWS = 1 };
 
 struct InferArgs {
@@ -239,7 +247,9 @@ struct InferArgs {
   int n_tiles;
   const unsigned char* wimg;  // [6][kImgBytes]
   const float* params;        // [6][kParams]
-  float* delta;               // [n_tiles * 128][6]
+  // [n_tiles * 128][6]: SRC_GRIDS the corrected values of the six
+  // components of each cell, SRC_ROWS the network outputs s * o
+  float* delta;
   const float* rows;          // SRC_ROWS: [n][54] normalised features
   int* err;
   unsigned long long wait_ns;
@@ -255,7 +265,7 @@ constexpr int kInfSmem = kInfOffBar + 16;
 constexpr int kInfTmemCols = 64;
 
 template <int SRC>
-__global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ InferArgs p) {
+__global__ void __launch_bounds__(128, 5) k_band_infer(const __grid_constant__ InferArgs p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* bufA = smem + kInfOffA;
   unsigned char* bufW = smem + kInfOffW;
@@ -300,10 +310,11 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
     }
     const int i = t * kTile + tid;
     float v[kInP];
+    float ctr[6];  // SRC_GRIDS: the cell's six components before the correction
     float s = 0.0f;
     if (cg.x >= 0) {
       if (SRC == SRC_GRIDS) {
-        s = gather(p.grids[cg.y], cg.x, face, v);
+        s = gather(p.grids[cg.y], cg.x, face, v, ctr);
         const float inv = 1.0f / s;
 #pragma unroll
         for (int k = 0; k < kIn; ++k) v[k] *= inv;
@@ -399,8 +410,17 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
     tc::ld16(lane_base, v);
     if (cg.x >= 0 && !timed) {
       float* d = p.delta + (size_t)i * kOut;
+      if (SRC == SRC_GRIDS) {
+        // X_c + s o (H rescaled by 1 / eta0), rounded as separate steps
 #pragma unroll
-      for (int o = 0; o < kOut; ++o) d[o] = s * v[o];
+        for (int o = 0; o < kOut; ++o) {
+          const float so = __fmul_rn(s, v[o]);
+          d[o] = __fadd_rn(ctr[o], o >= 3 ? __fmul_rn(so, 1.0f / kEta0) : so);
+        }
+      } else {
+#pragma unroll
+        for (int o = 0; o < kOut; ++o) d[o] = s * v[o];
+      }
     }
   }
   tc::fence_before_sync();
@@ -412,23 +432,28 @@ __global__ void __launch_bounds__(128) k_band_infer(const __grid_constant__ Infe
   if (tid < 32) tc::tmem_dealloc(tm, kInfTmemCols);
 }
 
-// X_c += delta (H rescaled); padding entries skipped.  The grid record is
+// X_c <- the corrected values the inference wrote (padding entries skipped).
+// A separate launch, because the stencils of other tiles read the
+// uncorrected outer cells; the inference formed X_c + s o from the values
+// it gathered, so the fields are only written here, never read (on z faces
+// every component of a cell is its own DRAM sector).  The grid record is
 // copied into registers once (through a reference into global memory every
-// store would force the field pointers to be reloaded), and all six fields
-// are read before any is written, so a thread's loads are in flight together.
-__global__ void k_band_apply(const GridRef* grids, const int2* cells, int n, const float* delta) {
+// store would force the field pointers to be reloaded).  If the inference
+// reported an error (a wait that gave up leaves tiles unwritten), nothing is
+// stored: the fields keep the plain Yee step.
+__global__ void k_band_apply(const GridRef* grids, const int2* cells, int n, const float* xnew,
+                             const int* err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (__ldcg(err) != 0) return;
   const int2 cg = cells[i];
   if (cg.x < 0) return;
   const GridRef g = grids[cg.y];
-  float d[kOut], f[6];
+  float d[kOut];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) d[c] = delta[(size_t)i * kOut + c];
+  for (int c = 0; c < 6; ++c) d[c] = xnew[(size_t)i * kOut + c];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) f[c] = g.f[c][cg.x];
-#pragma unroll
-  for (int c = 0; c < 6; ++c) g.f[c][cg.x] = __fadd_rn(f[c], c >= 3 ? d[c] * (1.0f / kEta0) : d[c]);
+  for (int c = 0; c < 6; ++c) g.f[c][cg.x] = d[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -458,7 +483,8 @@ __global__ void k_band_collect(const __grid_constant__ CollectArgs p) {
   while (e >= p.first[f + 1]) ++f;
   const int cell = p.cells[e];
   float v[kIn];
-  const float s = gather(p.t, cell, f, v);
+  float ctr[6];
+  const float s = gather(p.t, cell, f, v, ctr);
   const float inv = 1.0f / s;
   const long long row = p.base[f] + (e - p.first[f]);
   __nv_bfloat16* fr = p.feat[f] + row * kInP;
