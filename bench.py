@@ -417,11 +417,14 @@ def run_batch(args, world, rank, local, pg, steps=None, warmup=None, reflection=
     torch.cuda.set_device(local)
     n_grids, nsteps, _, wname = WORKLOADS["c5"]
     n_grids = getattr(args, "batch_grids", None) or n_grids
+    nsteps = getattr(args, "leapfrog_steps", None) or nsteps
     kinds = [k for k in getattr(args, "batch_kinds", "learned,cpml10,cpml4,pec").split(",") if k]
     if kinds[0] != "learned":
         raise SystemExit("--batch-kinds must start with learned")
     if n_grids != WORKLOADS["c5"][0]:
         wname = f"{wname}-first{n_grids}"
+    if nsteps != WORKLOADS["c5"][1]:
+        wname = f"{wname}-{nsteps}steps"
     # the 64 grids are bin-packed by cell count over the ranks (largest first
     # onto the least-loaded rank): a fixed total batch, so strong scaling
     all_cases = c5_cases(seed=5, n_grids=n_grids)
@@ -743,6 +746,8 @@ def main():
                     help="c5: grids whose reflection is measured against a padded reference")
     ap.add_argument("--batch-grids", type=int, default=None,
                     help="c5: run only the first N grids of the seeded 64 (profiling)")
+    ap.add_argument("--leapfrog-steps", type=int, default=None,
+                    help="c5: leapfrog steps per timed run instead of 1000 (profiling)")
     ap.add_argument("--batch-kinds", default="learned,cpml10,cpml4,pec",
                     help="c5: boundary variants to time, learned first (profiling)")
     ap.add_argument("--no-secondary", action="store_true",
