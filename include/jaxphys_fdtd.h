@@ -147,7 +147,8 @@ int jxf_grid3d_set_probes(jxf_grid3d* g, int32_t n, const int64_t* cell,
 /* Advance n_steps leapfrog steps; replaces one jax.lax.scan over `step`
  * (fdtd3d.py:280-393).  probe_out: DEVICE float32 [n_steps][n_probes] or
  * NULL.  Returns JXF_ERR_TIMEOUT if a bounded device wait gave up (checked
- * only when the call synchronises; see jxf_grid3d_check_error). */
+ * only when the call synchronises; see jxf_grid3d_check_error).  An x-slab
+ * (jxf_grid3d_create_slab) takes it only on the TMA path, one step per call. */
 int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stream);
 
 /* Adjoint (extension; the reference differentiates nothing in its FDTD,
@@ -181,7 +182,15 @@ int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_grad, float* g
  * and records its probes into probe_row.  Sources and probes take LOCAL cell
  * indices.  jxf_grid3d_plane copies one plane of one component between the
  * grid and a device buffer (to_buf != 0: grid -> buffer).  PERIODIC grids are
- * not decomposed. */
+ * not decomposed.
+ *
+ * With desc->path == JXF_PATH_TMA (nz % 4 == 0) the slab instead takes whole
+ * steps on the one-step TMA kernel, jxf_grid3d_step with n_steps = 1:
+ * before each, fill local plane x1-x0+1 with Ey, Ez of global plane x1 and
+ * local plane 0 with Ex, Ey, Ez of global plane x0-1 (the neighbours' edge
+ * planes of the current state).  The kernel recomputes H on local plane 0 as
+ * a bitwise replica of the previous rank's last plane (its psi included) and
+ * never updates E on a ghost plane.  Half steps are refused on such slabs. */
 int jxf_grid3d_create_slab(const jxf_grid3d_desc* desc, int32_t x0, int32_t x1,
                            jxf_grid3d** out);
 int jxf_grid3d_half_step(jxf_grid3d* g, int32_t half, float* probe_row, void* stream);

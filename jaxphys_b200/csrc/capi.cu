@@ -358,13 +358,30 @@ int build_generic_sources(jxf_grid3d* g) {
   return JXF_OK;
 }
 
+// Local planes [beg, end) that the one-step TMA pass marches over, in chunks
+// of x_chunk from beg (the kernel derives the same range from gx0 and x_hi):
+// every plane of a whole grid; the owned planes of an x-slab and its left
+// ghost plane (H recomputed there), unless that ghost lies outside the grid.
+void march_range(const jxf_grid3d* g, int& beg, int& end) {
+  beg = g->gx0 < 0 ? 1 : 0;
+  end = g->x_hi;
+}
+int march_chunks(const jxf_grid3d* g, int chunk) {
+  int beg, end;
+  march_range(g, beg, end);
+  return (end - beg + chunk - 1) / chunk;
+}
+
 // Per-block source lists for the TMA kernel: CSR over blocks, entries sorted
-// by plane, list order kept inside a plane (stable sort).
+// by plane, list order kept inside a plane (stable sort).  Sources on the
+// ghost planes of an x-slab belong to the neighbour and are left out.
 int build_tma_sources(jxf_grid3d* g) {
   const TmaConfig& c = tma_configs()[g->cfg];
-  const int ny = g->d.ny, nz = g->d.nz, nx = g->d.nx;
+  const int ny = g->d.ny, nz = g->d.nz;
   const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
-  const int nch = (nx + g->x_chunk - 1) / g->x_chunk;
+  int xbeg, xend;
+  march_range(g, xbeg, xend);
+  const int nch = march_chunks(g, g->x_chunk);
   const int nblk = ntz * nty * nch;
   std::vector<std::pair<int, int>> keyed;  // (block, source index)
   for (size_t i = 0; i < g->src_cell.size(); ++i) {
@@ -372,7 +389,8 @@ int build_tma_sources(jxf_grid3d* g) {
     const int z = (int)(cell % nz);
     const int y = (int)((cell / nz) % ny);
     const int x = (int)(cell / ((long long)nz * ny));
-    const int b = ((x / g->x_chunk) * nty + y / c.ty) * ntz + z / c.tz;
+    if (x < g->x_lo || x >= g->x_hi) continue;
+    const int b = (((x - xbeg) / g->x_chunk) * nty + y / c.ty) * ntz + z / c.tz;
     keyed.push_back({b, (int)i});
   }
   std::stable_sort(keyed.begin(), keyed.end(), [&](const auto& u, const auto& v) {
@@ -526,7 +544,7 @@ int launch_tma(jxf_grid3d* g, int cfg, int chunk, Step3D& p, int in_set, cudaStr
   p.x_chunk = chunk;
   p.ntiles_z = (g->d.nz + c.tz - 1) / c.tz;
   p.ntiles_y = (g->d.ny + c.ty - 1) / c.ty;
-  dim3 grid(p.ntiles_z, p.ntiles_y, (g->d.nx + chunk - 1) / chunk);
+  dim3 grid(p.ntiles_z, p.ntiles_y, march_chunks(g, chunk));
   if (list_count >= 0) grid = dim3(list_count, 1, 1);
   cudaLaunchConfig_t lc{};
   lc.gridDim = grid;
@@ -610,10 +628,11 @@ int tile_cpml_warps(const jxf_grid3d* g, const TmaConfig& c, int z0, int y0, boo
 }
 
 double shell_block_cost(const jxf_grid3d* g, const TmaConfig& c, int cw, int xb, int xe) {
-  const int nx = g->d.nx, warps = (c.threads + 31) / 32;
+  const int warps = (c.threads + 31) / 32;
   double cost = 0.0;
   for (int x = std::max(xb - 1, 0); x < xe; ++x) {
-    const double plane = in_slab(x, nx, g->P[0]) ? 2.0 * warps : 2.0 * cw + (warps - cw);
+    const bool xin = in_slab(x + g->gx0, g->gnx, g->P[0]);
+    const double plane = xin ? 2.0 * warps : 2.0 * cw + (warps - cw);
     cost += x < xb ? 0.5 * plane : plane;
   }
   return cost;
@@ -629,9 +648,11 @@ struct SplitLists {
 
 void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, SplitLists& out) {
   const TmaConfig& c = tma_configs()[cfg];
-  const int nx = g->d.nx, ny = g->d.ny, nz = g->d.nz;
+  const int ny = g->d.ny, nz = g->d.nz;
   const int ntz = (nz + c.tz - 1) / c.tz, nty = (ny + c.ty - 1) / c.ty;
-  const int nch = (nx + chunk - 1) / chunk;
+  int xbeg, xend;
+  march_range(g, xbeg, xend);
+  const int nch = march_chunks(g, chunk);
   struct Blk {
     double cost;
     int tz, ty, word;
@@ -642,12 +663,13 @@ void compute_split(const jxf_grid3d* g, int cfg, int chunk, bool axis_split, Spl
   for (int ch = 0; ch < nch; ++ch)
     for (int ty = 0; ty < nty; ++ty)
       for (int tz = 0; tz < ntz; ++tz) {
-        const int z0 = tz * c.tz, y0 = ty * c.ty, xb = ch * chunk;
-        const int xe = std::min(xb + chunk, nx);
+        const int z0 = tz * c.tz, y0 = ty * c.ty, xb = xbeg + ch * chunk;
+        const int xe = std::min(xb + chunk, xend);
         // cells of the tile, its halo row / column, and the warm-up plane
+        // (x in global planes)
         const bool cz = range_clear(z0 - 1, z0 + c.tz - 1, nz, g->P[2]);
         const bool cy = range_clear(y0 - 1, y0 + c.ty - 1, ny, g->P[1]);
-        const bool cx = range_clear(xb - 1, xe - 1, nx, g->P[0]);
+        const bool cx = range_clear(xb - 1 + g->gx0, xe - 1 + g->gx0, g->gnx, g->P[0]);
         const int touched = (cx ? 0 : 1) + (cy ? 0 : 1) + (cz ? 0 : 1);
         if (touched == 0) {
           parts[4].push_back({(double)(xe - std::max(xb - 1, 0)) * warps, tz, ty, ch});
@@ -1056,8 +1078,10 @@ int axis_split_override() {
 // Time every (config, chunk, axis split) on A -> B launches (the state in A
 // and the step counter are untouched, probes off) and keep the fastest.
 int autotune(jxf_grid3d* g, cudaStream_t st) {
-  const auto key =
-      std::make_tuple(g->d.nx, g->d.ny, g->d.nz, g->mode * 2 + (g->kappa ? 1 : 0), g->cb ? 1 : 0);
+  // (x-slabs tune apart from whole grids: they take no blocked passes)
+  const auto key = std::make_tuple(g->d.nx, g->d.ny, g->d.nz,
+                                   g->mode * 4 + (g->kappa ? 1 : 0) + (g->slab ? 2 : 0),
+                                   g->cb ? 1 : 0);
   const int split_env = axis_split_override();
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1074,9 +1098,10 @@ int autotune(jxf_grid3d* g, cudaStream_t st) {
   // JXF_TB: "off" keeps one step per launch; "cfg,chunk[,split]" pins the
   // two-level blocked launch shape
   const char* tb_env = std::getenv("JXF_TB");
-  const bool tb_off = tb_env && std::strcmp(tb_env, "off") == 0;
+  // (x-slabs take one step per pass: ghost planes are exchanged between steps)
+  const bool tb_off = (tb_env && std::strcmp(tb_env, "off") == 0) || g->slab;
   int tfc = -1, tfk = -1, tfs = -1;
-  const bool tb_forced = tb_env && !tb_off &&
+  const bool tb_forced = tb_env && !tb_off && !g->slab &&
                          std::sscanf(tb_env, "%d,%d,%d", &tfc, &tfk, &tfs) >= 2 && tfc >= 0 &&
                          tfc < (int)tb_configs().size() && tfk >= 1;
   const char* env = std::getenv("JXF_AUTOTUNE");
@@ -1286,7 +1311,6 @@ int jxf_grid3d_create_slab(const jxf_grid3d_desc* desc, int32_t x0, int32_t x1,
     return fail(JXF_ERR_INVALID, "x-slab decomposition does not support PERIODIC boundaries");
   jxf_grid3d_desc d = *desc;
   d.nx = x1 - x0 + 2;  // owned planes plus one ghost plane on each side
-  d.path = JXF_PATH_GENERIC;
   return create3d(d, desc->nx, x0 - 1, 1, x1 - x0 + 1, true, out);
 }
 
@@ -1540,6 +1564,8 @@ int jxf_grid3d_set_blocked(jxf_grid3d* g, int32_t cfg, int32_t x_chunk) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
   if (g->path != JXF_PATH_TMA) return fail(JXF_ERR_INVALID, "grid does not use the TMA path");
   if (cfg >= (int)tb_configs().size()) return fail(JXF_ERR_INVALID, "blocked cfg out of range");
+  if (cfg >= 0 && g->slab)
+    return fail(JXF_ERR_INVALID, "x-slab grids take one step per pass (no blocked passes)");
   if (cfg >= 0 && x_chunk < 1) return fail(JXF_ERR_INVALID, "x_chunk must be >= 1");
   if (g->cfg < 0) TRY(heuristic_tune(g));  // one-step shape for odd remainders
   g->tb = cfg < 0 ? -1 : cfg;
@@ -1664,8 +1690,12 @@ static int gather_probes(jxf_grid3d* g, int set, float* out, cudaStream_t st) {
 
 int jxf_grid3d_step(jxf_grid3d* g, int32_t n_steps, float* probe_out, void* stream) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
-  if (g->slab)
-    return fail(JXF_ERR_INVALID, "x-slab grids advance with jxf_grid3d_half_step (ghost exchange)");
+  if (g->slab && g->path != JXF_PATH_TMA)
+    return fail(JXF_ERR_INVALID, "x-slab grids on the generic path advance with "
+                "jxf_grid3d_half_step (ghost exchange)");
+  if (g->slab && n_steps > 1)
+    return fail(JXF_ERR_INVALID, "an x-slab grid takes one step per call (its ghost planes are "
+                "exchanged between steps)");
   if (n_steps < 0) return fail(JXF_ERR_INVALID, "n_steps must be >= 0");
   if (n_steps == 0) return JXF_OK;
   if (!g->src_cell.empty()) {
@@ -1774,6 +1804,9 @@ int jxf_grid3d_half_step_part(jxf_grid3d* g, int32_t half, int32_t part, float* 
                               void* stream) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
   if (!g->slab) return fail(JXF_ERR_INVALID, "half steps are for x-slab grids");
+  if (g->path != JXF_PATH_GENERIC)
+    return fail(JXF_ERR_INVALID, "half steps run on generic-path x-slabs (a TMA x-slab takes "
+                "whole steps: jxf_grid3d_step)");
   if (half != 0 && half != 1) return fail(JXF_ERR_INVALID, "half must be 0 (H) or 1 (E)");
   if (part < 0 || part > 2) return fail(JXF_ERR_INVALID, "part must be 0, 1 or 2");
   if (part == 0) return jxf_grid3d_half_step(g, half, probe_row, stream);
@@ -1834,6 +1867,9 @@ int jxf_grid3d_half_step_part(jxf_grid3d* g, int32_t half, int32_t part, float* 
 int jxf_grid3d_half_step(jxf_grid3d* g, int32_t half, float* probe_row, void* stream) {
   if (!g) return fail(JXF_ERR_INVALID, "null handle");
   if (!g->slab) return fail(JXF_ERR_INVALID, "half steps are for x-slab grids");
+  if (g->path != JXF_PATH_GENERIC)
+    return fail(JXF_ERR_INVALID, "half steps run on generic-path x-slabs (a TMA x-slab takes "
+                "whole steps: jxf_grid3d_step)");
   if (half != 0 && half != 1) return fail(JXF_ERR_INVALID, "half must be 0 (H) or 1 (E)");
   if (half == 1 && !g->src_cell.empty()) {
     int max_w = 0;
@@ -3857,6 +3893,8 @@ extern "C" int jxf_grid3d_run_noalloc(const jxf_noalloc_desc* desc, float* const
   p.nx = d.nx;
   p.ny = d.ny;
   p.nz = d.nz;
+  p.gnx = d.nx;  // a whole grid: gx0 = x_lo = 0
+  p.x_hi = d.nx;
   p.a = (float)(dt / (kMu0 * d.dx));
   p.cb_const = (float)(dt / (kEps0 * d.dx));
   p.cb = cb;

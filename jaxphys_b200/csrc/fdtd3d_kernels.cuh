@@ -599,8 +599,16 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
   int ty = tid / TZ;
   if (CPML && RY == 1 && slab_first)
     slab_first_cell<TZ, TY>(tid, z0, y0, nz, ny, p.pml.P[1], p.pml.P[2], AY, AZ, tx, ty);
-  const int xb = ci * p.x_chunk;
-  const int xe = min(xb + p.x_chunk, nx);
+  // Planes marched: a whole grid marches over all of them.  An x-slab of a
+  // decomposed grid marches over its owned planes [x_lo, x_hi) and the left
+  // ghost plane before them, where H is recomputed as a bitwise replica of
+  // the neighbour's last plane and E is not updated (the neighbour's E
+  // arrives there before each step); on the first slab that ghost plane is
+  // outside the grid and is skipped.  Boundaries, coefficient tables, x-slab
+  // psi and damping use the global plane x + gx0.
+  const int xbeg = p.gx0 < 0 ? 1 : 0;
+  const int xb = xbeg + ci * p.x_chunk;
+  const int xe = min(xb + p.x_chunk, p.x_hi);
   const int qs = xb > 0 ? xb - 1 : 0;  // first plane staged
   const int qe = min(xe, nx - 1);      // last plane staged
   const int nload = qe - qs + 1;
@@ -728,7 +736,7 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
 #define PSH(buf, k) PSh[((buf) * 4 + (k)) * NH + tid]
   // Prefetch psi_in of plane q into buffer `buf` (this thread's cells only).
   auto issue_psi = [&](int q, int buf) {
-    const int imq = slab_map(q, nx, p.pml.P[0]);
+    const int imq = slab_map(q + p.gx0, p.gnx, p.pml.P[0]);
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       if (iny[r]) {
@@ -819,18 +827,19 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
 #define H_AT(c, yy, zc) Hs[(c) * L::H_STRIDE + (yy) * HW + (zc)]
 #define HN_AT(c, yy, zc) Hn[(c) * L::HN_STRIDE + (yy) * NW + (zc)]
     const bool warm = (x < xb);
+    const int xg = x + p.gx0;  // global plane
     int imx = -1;
     float xbh = 1.f, xch = 0.f, xbe = 1.f, xce = 0.f, xikh = 1.f, xike = 1.f;
     if (CPML) {
-      imx = AX ? slab_map(x, nx, p.pml.P[0]) : -1;
+      imx = AX ? slab_map(xg, p.gnx, p.pml.P[0]) : -1;
       if (imx >= 0) {
-        xbh = __ldg(p.pml.tab[0][TAB_BH] + x);
-        xch = __ldg(p.pml.tab[0][TAB_CH] + x);
-        xbe = __ldg(p.pml.tab[0][TAB_BE] + x);
-        xce = __ldg(p.pml.tab[0][TAB_CE] + x);
+        xbh = __ldg(p.pml.tab[0][TAB_BH] + xg);
+        xch = __ldg(p.pml.tab[0][TAB_CH] + xg);
+        xbe = __ldg(p.pml.tab[0][TAB_BE] + xg);
+        xce = __ldg(p.pml.tab[0][TAB_CE] + xg);
         if (KAPPA) {
-          xikh = __ldg(p.pml.tab[0][TAB_IKH] + x);
-          xike = __ldg(p.pml.tab[0][TAB_IKE] + x);
+          xikh = __ldg(p.pml.tab[0][TAB_IKH] + xg);
+          xike = __ldg(p.pml.tab[0][TAB_IKE] + xg);
         }
       }
     }
@@ -854,8 +863,8 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
       ezr[r] = ezc;
       float hx = H_AT(0, yy, zz), hy = H_AT(1, yy, zz), hz = H_AT(2, yy, zz);
       const bool ux = !warm && y < ny - 1 && z < nz - 1;
-      const bool uy = x < nx - 1 && z < nz - 1 && y < ny;
-      const bool uz = x < nx - 1 && y < ny - 1 && z < nz;
+      const bool uy = xg < p.gnx - 1 && z < nz - 1 && y < ny;
+      const bool uz = xg < p.gnx - 1 && y < ny - 1 && z < nz;
       const float dyEz = fsub(E_AT(2, yy + 1, zz), ezc), dzEy = fsub(E_AT(1, yy, zz + 1), eyc);
       const float dzEx = fsub(E_AT(0, yy, zz + 1), exc), dxEz = fsub(EN_AT(2, yy, zz), ezc);
       const float dxEy = fsub(EN_AT(1, yy, zz), eyc), dyEx = fsub(E_AT(0, yy + 1, zz), exc);
@@ -916,7 +925,7 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
             else
               hx = h_plain(hx, a, d1, d2);
           }
-          if (x < nx - 1) {
+          if (xg < p.gnx - 1) {
             const float d1 = fsub(EN_AT(1, 0, zb), eyc), d2 = fsub(E_AT(0, 1, zb), exc);
             if (CPML)
               hz = h_sel<KAPPA>(hz, a, d1, d2, inx, inyh, pnext(inx, xbh, xch, PSH(pb, 2), d1),
@@ -943,7 +952,7 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
             else
               hx = h_plain(hx, a, d1, d2);
           }
-          if (x < nx - 1) {
+          if (xg < p.gnx - 1) {
             const float d1 = fsub(E_AT(0, yy, 4), exc), d2 = fsub(EN_AT(2, yy, 3), ezc);
             if (CPML)
               hy = h_sel<KAPPA>(hy, a, d1, d2, inzh, inx, pnext(inzh, hzb, hzc, PSH(pb, 2), d1),
@@ -983,7 +992,10 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
         float ex = exr[r], ey = eyr[r], ez = ezr[r];
         const float hxc = hxr[r], hyc = hyr[r], hzc = hzr[r];
         const float cb = cbr[r];
-        const bool ux = y >= 1 && z >= 1, uy = x >= 1 && z >= 1, uz = x >= 1 && y >= 1;
+        // E is not updated on a ghost plane (x < x_lo): it keeps its input
+        const bool ep = x >= p.x_lo;
+        const bool ux = ep && y >= 1 && z >= 1, uy = ep && xg >= 1 && z >= 1,
+                   uz = ep && xg >= 1 && y >= 1;
         const float dyHz = fsub(hzc, HN_AT(2, yy - 1, zn)), dzHy = fsub(hyc, HN_AT(1, yy, zn - 1));
         const float dzHx = fsub(hxc, HN_AT(0, yy, zn - 1)), dxHz = fsub(hzc, hz_prev[r]);
         const float dxHy = fsub(hyc, hy_prev[r]), dyHx = fsub(hxc, HN_AT(0, yy - 1, zn));
@@ -1016,9 +1028,9 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
           if (uy) ey = e_plain(ey, cb, dzHx, dxHz);
           if (uz) ez = e_plain(ez, cb, dxHy, dyHx);
         }
-        if (MODE == MODE_ABSORB && own) {
+        if (MODE == MODE_ABSORB && own && ep) {
           const float f =
-              fmul(fmul(__ldg(p.damp[0] + x), __ldg(p.damp[1] + y)), __ldg(p.damp[2] + z));
+              fmul(fmul(__ldg(p.damp[0] + xg), __ldg(p.damp[1] + y)), __ldg(p.damp[2] + z));
           ex = fmul(ex, f);
           ey = fmul(ey, f);
           ez = fmul(ez, f);

@@ -21,6 +21,13 @@ plane a neighbour needs, posts the swap, updates the remaining planes while
 the planes cross the link, and waits for the swap only before the half-step
 that reads the ghost plane.  Probe traces are all-reduced so every rank
 returns the full trace.
+
+With ``path="tma"`` (nz % 4 == 0) each slab instead takes whole steps on the
+one-step TMA kernel (``jxf_grid3d_step``, one step per call).  The kernel
+recomputes H on the low ghost plane as a bitwise replica of the previous
+rank's last plane and never updates E on a ghost plane.  So before each step
+only E planes of the current state cross: Ey, Ez of the next rank's first
+plane, and Ex, Ey, Ez of the previous rank's last plane.
 """
 
 from __future__ import annotations
@@ -51,7 +58,8 @@ def slab_ranges(nx: int, world: int) -> list[tuple[int, int]]:
 class CudaSlabStepper:
     """Local part of the grid on this rank's GPU (the product path)."""
 
-    def __init__(self, size, x0, x1, dx, dt, boundary, pml_layers, cpml: CPMLSpec, device: int):
+    def __init__(self, size, x0, x1, dx, dt, boundary, pml_layers, cpml: CPMLSpec, device: int,
+                 path: int = nat.PATH_GENERIC):
         import torch
 
         self.torch = torch
@@ -61,7 +69,7 @@ class CudaSlabStepper:
         d = nat.Grid3DDesc(nx=nx, ny=ny, nz=nz, dx=float(dx), dt=float(dt), boundary=boundary,
                            pml_layers=int(pml_layers), cpml_order=float(cpml.order),
                            cpml_r0=float(cpml.r0), cpml_kappa_max=float(cpml.kappa_max),
-                           cpml_alpha_max=float(cpml.alpha_max), path=nat.PATH_GENERIC,
+                           cpml_alpha_max=float(cpml.alpha_max), path=int(path),
                            device=int(device))
         h = C.c_void_p()
         lib = nat.load()
@@ -71,6 +79,8 @@ class CudaSlabStepper:
         self.lib = lib
         self.device = self.dev
         self.dtype = torch.float32
+        # a TMA slab takes whole leapfrog steps (one fused pass per step)
+        self.whole_steps = int(path) == nat.PATH_TMA
 
     def close(self):
         if self.h is not None:
@@ -119,6 +129,12 @@ class CudaSlabStepper:
             self.h, half, part, None if probe_row is None else probe_row.data_ptr(),
             nat.stream_handle()), "jxf_grid3d_half_step_part")
 
+    def step(self, probe_row=None):
+        """One whole leapfrog step (TMA slabs; ghost E planes exchanged before)."""
+        nat.check(self.lib.jxf_grid3d_step(
+            self.h, 1, None if probe_row is None else probe_row.data_ptr(),
+            nat.stream_handle()), "jxf_grid3d_step")
+
     def new_probe_buffer(self, n_steps: int, n_local: int):
         return self.torch.zeros((n_steps, n_local), dtype=self.torch.float32, device=self.dev)
 
@@ -143,7 +159,7 @@ class DistributedGrid3D:
 
     def __init__(self, size, resolution=0.01, boundary="absorbing", pml_layers=8, *,
                  cpml: CPMLSpec | None = None, group=None, device: int | None = None,
-                 stepper_factory=None, overlap: bool = True):
+                 stepper_factory=None, overlap: bool = True, path: str = "generic"):
         import torch.distributed as dist
 
         self.dist = dist
@@ -155,6 +171,11 @@ class DistributedGrid3D:
             raise ConfigurationError(f"Grid must be at least 8x8x8, got {size}")
         if boundary not in ("absorbing", "pec", "cpml"):
             raise ConfigurationError(f"decomposed grids support absorbing, pec and cpml, not {boundary!r}")
+        if path not in ("generic", "tma"):
+            raise ConfigurationError(f"path must be 'generic' or 'tma', not {path!r}")
+        if path == "tma" and self.size[2] % 4 != 0:
+            raise ConfigurationError(f"the TMA path needs nz % 4 == 0 (got nz = {self.size[2]})")
+        self.path = path
         self.dx = resolution
         self.boundary = boundary
         self.pml_layers = pml_layers
@@ -171,8 +192,10 @@ class DistributedGrid3D:
 
             dev = device if device is not None else torch.cuda.current_device()
 
+            kind = nat.PATH_TMA if path == "tma" else nat.PATH_GENERIC
+
             def stepper_factory(**kw):
-                return CudaSlabStepper(device=dev, **kw)
+                return CudaSlabStepper(device=dev, path=kind, **kw)
 
         self.st = stepper_factory(size=self.size, x0=self.x0, x1=self.x1, dx=self.dx, dt=self.dt,
                                   boundary=_BOUNDARY[boundary], pml_layers=pml_layers,
@@ -324,10 +347,23 @@ class DistributedGrid3D:
             self._wave_len = 2 * (self.step_count + n_steps)
             self.st.set_waveforms(wf.build_table(keys, self._wave_len, self.dt, 0.0))
         buf = self.st.new_probe_buffer(n_steps, len(self.own_probes))
-        if self.overlap:
+        if getattr(self.st, "whole_steps", False):
+            # TMA slab: one fused pass per step.  Before it, the ghost E planes
+            # of the current state: Ey, Ez of the next rank's first plane
+            # (H at my last owned plane differences E at x+1) and Ex, Ey, Ez
+            # of the previous rank's last plane (my low ghost plane, where H
+            # is recomputed as a bitwise replica of that rank's last plane).
+            for k in range(n_steps):
+                row = buf[k] if len(self.own_probes) else None
+                hi = self._start_exchange((1, 2), 1, -1)
+                lo = self._start_exchange((0, 1, 2), self.nloc, +1)
+                self._finish_exchange(hi, (1, 2), self.nloc + 1)
+                self._finish_exchange(lo, (0, 1, 2), 0)
+                self.st.step(row)
+        elif self.overlap:
             # the E ghost plane of the current state
             self._exchange((1, 2), 1, self.nloc + 1, -1)
-        for k in range(n_steps):
+        for k in range(n_steps if not getattr(self.st, "whole_steps", False) else 0):
             row = buf[k] if len(self.own_probes) else None
             if not self.overlap:
                 # Ey, Ez of the next rank's first plane -> my high ghost plane

@@ -31,7 +31,7 @@ class NumpySlabStepper:
         self.device = torch.device("cpu")
         self.dtype = torch.float64
         self.src, self.probes = [], []
-        self.step = 0
+        self.n_step = 0
 
     def close(self):
         pass
@@ -51,7 +51,7 @@ class NumpySlabStepper:
     def reset(self):
         for a in self.f:
             a[...] = 0.0
-        self.step = 0
+        self.n_step = 0
 
     def get_plane(self, comp, plane):
         return torch.from_numpy(self.f[comp][plane].copy())
@@ -112,13 +112,27 @@ class NumpySlabStepper:
         plane = self.shape[1] * self.shape[2]
         for cell, comp, amp, row in self.src:
             if lo <= cell // plane < hi:
-                flat[comp][cell] += amp * self.wave[row, self.step]
+                flat[comp][cell] += amp * self.wave[row, self.n_step]
         if not final:
             return
         if probe_row is not None:
             for k, (cell, comp) in enumerate(self.probes):
                 probe_row[k] = float(flat[comp][cell])
-        self.step += 1
+        self.n_step += 1
+
+
+class NumpyWholeStepSlabStepper(NumpySlabStepper):
+    """Whole steps as a TMA slab takes them: H on the owned planes and on the
+    low ghost plane (a replica of the previous rank's last plane, from the
+    ghost E plane received before the step; skipped when that plane lies
+    outside the grid), then E on the owned planes only."""
+
+    whole_steps = True
+
+    def step(self, probe_row=None):
+        beg = 0 if self.x0 >= 1 else 1
+        self.half_step(0, None, beg, self.nloc + 1)
+        self.half_step(1, probe_row)
 
 
 def free_port() -> int:

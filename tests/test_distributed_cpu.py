@@ -29,17 +29,18 @@ def _sources(dt):
 PROBES = [(6, 5, 9, "ez"), (2, 8, 2, "hy"), (11, 3, 7, "ex"), (4, 4, 4, "hz")]
 
 
-def _worker(rank, world, port, boundary, out_path, overlap=True):
+def _worker(rank, world, port, boundary, out_path, overlap=True, whole=False):
     import torch.distributed as dist
 
-    from dist_helpers import NumpySlabStepper
+    from dist_helpers import NumpySlabStepper, NumpyWholeStepSlabStepper
     from jaxphys_b200.em.distributed import DistributedGrid3D
 
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world)
     try:
         g = DistributedGrid3D(SIZE, resolution=1.0, boundary=boundary, pml_layers=3,
-                              stepper_factory=lambda **kw: NumpySlabStepper(**kw),
+                              stepper_factory=lambda **kw: (NumpyWholeStepSlabStepper(**kw) if whole
+                                                            else NumpySlabStepper(**kw)),
                               overlap=overlap)
         assert g.overlap == overlap
         for s in _sources(g.dt):
@@ -59,15 +60,19 @@ def _worker(rank, world, port, boundary, out_path, overlap=True):
 
 @pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("boundary", ["absorbing", "pec"])
-@pytest.mark.parametrize("overlap", [True, False])
-def test_slab_decomposition_matches_oracle(world, boundary, overlap):
-    """Both schedules: plain (exchange, then the whole half-step) and
-    overlapped (the neighbour's plane first, the exchange during the rest)."""
+@pytest.mark.parametrize("schedule", ["overlap", "plain", "whole"])
+def test_slab_decomposition_matches_oracle(world, boundary, schedule):
+    """The three schedules: half steps plain (exchange, then the whole
+    half-step) and overlapped (the neighbour's plane first, the exchange
+    during the rest), and the whole steps of TMA slabs (E ghost planes of
+    both neighbours exchanged, then H including the low ghost plane's
+    replica, then E on the owned planes)."""
     from dist_helpers import free_port
 
+    overlap, whole = schedule != "plain", schedule == "whole"
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "r.npz")
-        mp.start_processes(_worker, args=(world, free_port(), boundary, out, overlap),
+        mp.start_processes(_worker, args=(world, free_port(), boundary, out, overlap, whole),
                            nprocs=world,
                            join=True, start_method="spawn")
         res = np.load(out)
