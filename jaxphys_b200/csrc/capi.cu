@@ -3601,25 +3601,61 @@ int ensure_buf(T** p, size_t* cap, size_t count, int64_t* tally) {
   return JXF_OK;
 }
 
+// Several device-to-device copies of float arrays in one launch (the
+// recompute of an adjoint segment keeps H and the E psi after every step:
+// one launch instead of one copy per array).
+struct CopyList {
+  const float* src[18];
+  float* dst[18];
+  long long end[18];  // cumulative element counts
+  int n;
+};
+__global__ void k_copy_many(const __grid_constant__ CopyList c) {
+  const long long total = c.end[c.n - 1];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    int k = 0;
+    while (i >= c.end[k]) ++k;
+    const long long j = i - (k ? c.end[k - 1] : 0);
+    c.dst[k][j] = c.src[k][j];
+  }
+}
+struct CopyBatch {
+  CopyList c{};
+  void add(float* dst, const float* src, size_t n) {
+    if (n == 0) return;
+    c.src[c.n] = src;
+    c.dst[c.n] = dst;
+    c.end[c.n] = (c.n ? c.end[c.n - 1] : 0) + (long long)n;
+    ++c.n;
+  }
+  int launch(cudaStream_t st) {
+    if (c.n == 0) return JXF_OK;
+    const long long total = c.end[c.n - 1];
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
+    k_copy_many<<<blocks, 256, 0, st>>>(c);
+    CUDA_TRY(cudaGetLastError());
+    return JXF_OK;
+  }
+};
+
 // copy the current state (fields + psi) to / from one checkpoint slot
 int ckpt_copy(jxf_grid3d* g, float* slot, bool save, cudaStream_t st) {
   const size_t n = (size_t)g->n;
   size_t off = 0;
+  CopyBatch cb;
   for (int k = 0; k < 6; ++k) {
     float* f = g->f[g->cur][k];
-    CUDA_TRY(cudaMemcpyAsync(save ? slot + off : f, save ? f : slot + off, n * 4,
-                             cudaMemcpyDeviceToDevice, st));
+    cb.add(save ? slot + off : f, save ? f : slot + off, n);
     off += n;
   }
   for (int k = 0; k < PSI_COUNT; ++k) {
     const size_t sz = psi_size(g, k);
-    if (!sz) continue;
     float* q = g->psi[g->cur][k];
-    CUDA_TRY(cudaMemcpyAsync(save ? slot + off : q, save ? q : slot + off, sz * 4,
-                             cudaMemcpyDeviceToDevice, st));
+    cb.add(save ? slot + off : q, save ? q : slot + off, sz);
     off += sz;
   }
-  return JXF_OK;
+  return cb.launch(st);
 }
 
 }  // namespace
@@ -3722,18 +3758,17 @@ extern "C" int jxf_grid3d_adjoint_backward(jxf_grid3d* g, const float* probe_gra
       TRY(jxf_grid3d_step(g, 1, nullptr, stream));
       float* slot = g->adj_sg + (size_t)k * g->adj_segstate;
       size_t off = 0;
+      CopyBatch cb;
       for (int c = 0; c < 3; ++c) {
-        CUDA_TRY(cudaMemcpyAsync(slot + off, g->f[g->cur][3 + c], n * 4,
-                                 cudaMemcpyDeviceToDevice, st));
+        cb.add(slot + off, g->f[g->cur][3 + c], n);
         off += n;
       }
       for (int q = PSI_EXY; q < PSI_COUNT; ++q) {
         const size_t sz = psi_size(g, q);
-        if (!sz) continue;
-        CUDA_TRY(cudaMemcpyAsync(slot + off, g->psi[g->cur][q], sz * 4, cudaMemcpyDeviceToDevice,
-                                 st));
+        cb.add(slot + off, g->psi[g->cur][q], sz);
         off += sz;
       }
+      TRY(cb.launch(st));
     }
     // adjoint steps, last to first
     for (int k = len - 1; k >= 0; --k) {

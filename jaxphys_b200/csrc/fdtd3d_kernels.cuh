@@ -845,6 +845,7 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
     }
     const bool inx = imx >= 0;
 
+
     // ---------------- H^{n+1/2} on the tile (registers + Hn) ----------------
     float exr[RY], eyr[RY], ezr[RY], hxr[RY], hyr[RY], hzr[RY], cbr[RY];
 #pragma unroll
@@ -1039,25 +1040,48 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
         eyo[r] = ey;
         ezo[r] = ez;
       }
-      // soft sources of plane x (uniform loop: every thread reads each entry)
-      while (sp < se) {
-        const SrcEntry e = p.src[sp];
-        if (e.x != x) break;
-        const int yl_e = e.off / TZ;
-        const int tz_e = e.off - yl_e * TZ;
+      // soft sources of plane x, in list order; a thread adds the entries of
+      // its own cell
+      auto add_src = [&](int off, int comp, float v) {
+        const int yl_e = off / TZ;
+        const int tz_e = off - yl_e * TZ;
         if (tz_e == tx && (yl_e % TYT) == ty) {
           const int r_e = yl_e / TYT;
-          const float v = fmul(e.amp, p.wave[(long long)e.wave * p.wave_len + step]);
 #pragma unroll
           for (int r = 0; r < RY; ++r) {
             if (r == r_e) {
-              if (e.comp == 0) exo[r] = fadd(exo[r], v);
-              else if (e.comp == 1) eyo[r] = fadd(eyo[r], v);
+              if (comp == 0) exo[r] = fadd(exo[r], v);
+              else if (comp == 1) eyo[r] = fadd(eyo[r], v);
               else ezo[r] = fadd(ezo[r], v);
             }
           }
         }
-        ++sp;
+      };
+      // The block's entries are sorted by plane and those of plane x come
+      // first: lane k of every warp loads entry sp + k with its waveform
+      // sample (two round trips per 32 entries instead of two per entry) and
+      // the warp walks them in list order through shuffles.  sp < se is the
+      // same in every thread of the block.
+      while (sp < se) {
+        const int k = sp + (tid & 31);
+        bool here = false;
+        int s_off = 0, s_comp = 0;
+        float s_v = 0.0f;
+        if (k < se) {
+          const SrcEntry e = p.src[k];
+          here = e.x == x;
+          if (here) {
+            s_off = e.off;
+            s_comp = e.comp;
+            s_v = fmul(e.amp, p.wave[(long long)e.wave * p.wave_len + step]);
+          }
+        }
+        const int s_n = __popc(__ballot_sync(0xffffffffu, here));  // lanes 0 .. s_n-1
+        for (int j = 0; j < s_n; ++j)
+          add_src(__shfl_sync(0xffffffffu, s_off, j), __shfl_sync(0xffffffffu, s_comp, j),
+                  __shfl_sync(0xffffffffu, s_v, j));
+        sp += s_n;
+        if (s_n < 32) break;
       }
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
