@@ -3622,14 +3622,20 @@ __global__ void k_copy_many(const __grid_constant__ CopyList c) {
 }
 struct CopyBatch {
   CopyList c{};
+  bool overflow = false;
   void add(float* dst, const float* src, size_t n) {
     if (n == 0) return;
+    if (c.n == (int)(sizeof(c.src) / sizeof(c.src[0]))) {
+      overflow = true;
+      return;
+    }
     c.src[c.n] = src;
     c.dst[c.n] = dst;
     c.end[c.n] = (c.n ? c.end[c.n - 1] : 0) + (long long)n;
     ++c.n;
   }
   int launch(cudaStream_t st) {
+    if (overflow) return fail(JXF_ERR_INVALID, "internal: more than 18 arrays in one copy batch");
     if (c.n == 0) return JXF_OK;
     const long long total = c.end[c.n - 1];
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);

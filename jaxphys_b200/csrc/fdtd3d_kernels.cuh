@@ -566,7 +566,11 @@ __device__ __forceinline__ void slab_first_cell(int t, int z0, int y0, int nz, i
 // One block of work: the tile (tzi, tyi) over x chunk ci.  Called by the
 // single-grid kernel (one block per work item) and by the batch kernel (a
 // persistent block looping over the items of many grids).
-template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA, int AXES = 7>
+// WSRC: sources of a plane fetched by whole warps (single grids, where one
+// block may hold a plane source); the persistent batch kernel keeps the
+// per-entry loop, which measured faster there (its grids hold point sources).
+template <int TZ, int TY, int RY, int STAGES, int MODE, bool CBARR, bool KAPPA, int AXES = 7,
+          bool WSRC = true>
 __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, int tzi, int tyi,
                                           int ci, bool slab_first, long long step) {
   constexpr bool CPML = (MODE == MODE_CPML);
@@ -1062,7 +1066,7 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
       // sample (two round trips per 32 entries instead of two per entry) and
       // the warp walks them in list order through shuffles.  sp < se is the
       // same in every thread of the block.
-      while (sp < se) {
+      while (WSRC && sp < se) {
         const int k = sp + (tid & 31);
         bool here = false;
         int s_off = 0, s_comp = 0;
@@ -1082,6 +1086,12 @@ __device__ __forceinline__ void tma_block(const Step3D& p, const Maps3D& maps, i
                   __shfl_sync(0xffffffffu, s_v, j));
         sp += s_n;
         if (s_n < 32) break;
+      }
+      while (!WSRC && sp < se) {  // one entry at a time
+        const SrcEntry e = p.src[sp];
+        if (e.x != x) break;
+        add_src(e.off, e.comp, fmul(e.amp, p.wave[(long long)e.wave * p.wave_len + step]));
+        ++sp;
       }
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
@@ -1205,7 +1215,7 @@ __global__ void __launch_bounds__(TZ*(TY / RY))
       }
       if (CBARR) tensormap_acquire(&m.cb);
     }
-    tma_block<TZ, TY, RY, STAGES, MODE, CBARR, KAPPA, AXES>(
+    tma_block<TZ, TY, RY, STAGES, MODE, CBARR, KAPPA, AXES, false>(
         a.params[k], m, w.y, w.z, w.w & BLK_CHUNK_MASK, (w.w & BLK_SLAB_FIRST) != 0, a.step);
     __syncthreads();  // every wait of the item is over
     if (threadIdx.x == 0)
